@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""bench.py -- Mzone-updates/s at 256^3 including self-gravity.
+
+Workload (default): the 256^3 stellar octant explosion -- n=3 Lane-Emden star
+(M=1, R=0.4, gamma 5/3) in the reference's STELLAR_OCTANT_EXPLOSION_3D layout
+(reflective min faces, outflow max faces), 1% log-normal density noise from
+the reference's seeded LCG, thermal energy 1.0 inside r < 0.02 R, multipole
+boundary to l=8, every step's Poisson solve to the 1e-8 update norm.  Inputs
+are generated on the host (synthetic, seeded) and uploaded once; W warm-up
+steps (the first one includes the cold-start Poisson solve) are followed by K
+timed steps.
+
+One step = one godunov_step_3d of the reference (hydro_solver_3d.c:637-811):
+gravity solve, CFL dt, fused flux/update/source, boundaries.
+
+Arms:
+  (default)          this library's fastest configuration (FP32 hydro, mixed
+                     precision Poisson, learned warm start when weights exist)
+  --variant fp64     the FP64 path that is bit-identical to the reference
+  --impl reference   the reference's own C code (oracle/_ref, built from the
+                     reference sources) on the host CPU, one core (it is
+                     serial), on a bounded sample of each step
+
+Multi-GPU: the step does not shard (one grid per GPU in the reference), so
+--gpus N runs N independent replicas, one per rank; value = zones all ranks
+updated / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mzone-updates/s at 256^3 incl. gravity"
+UNIT = "Mzone-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="best", choices=["best", "fp32", "fp64", "fp64_tree"])
+    ap.add_argument("--n", type=int, default=256, help="grid cells per side")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local, dist
+
+
+def reduce_max(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def make_workload(n):
+    from hydrocode_astro1_b200 import problems
+    return problems.octant_explosion(n)
+
+
+def solver_kwargs(p, variant, device):
+    import hydrocode_astro1_b200 as hc
+    kw = dict(lo=p["lo"], hi=p["hi"], gamma=p["gamma"], G=p["G"], bc=p["bc"], lmax=p["lmax"],
+              cfl=p["cfl"], tol=1e-8, max_iter=2_000_000, omega=1.5, device=device)
+    if variant == "fp64":
+        kw.update(precision=hc.FP64, lmax=p["lmax"], moment_order=hc.MOMENTS_TREE)
+    elif variant == "fp64_tree":
+        kw.update(precision=hc.FP64, moment_order=hc.MOMENTS_TREE)
+    else:
+        kw.update(precision=hc.FP32, moment_order=hc.MOMENTS_TREE)
+    return kw
+
+
+def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
+    """Warm up, then time `steps` steps with CUDA events on the solver's stream."""
+    import hydrocode_astro1_b200 as hc
+    s = hc.HydroSolver3D(p["shape"], **solver_kwargs(p, variant, device))
+    s.set_state(q0)
+    warm_iters = []
+    for _ in range(warmup):
+        s.step(1)
+        warm_iters.append(s.diagnostics()["last_iterations"])
+    s.timing(reset=True)
+    iters = []
+    barrier(dist)
+    s.sync()
+    if clocks:
+        clocks.start()
+    s.timer_start()
+    dts = []
+    d0 = s.diagnostics()["total_iterations"]
+    for _ in range(steps):
+        dts.append(float(s.step(1)[0]))
+        iters.append(s.diagnostics()["last_iterations"])
+    ms = s.timer_stop()
+    ck = clocks.stop() if clocks else None
+    tm = s.timing()
+    d = s.diagnostics()
+    return dict(solver=s, ms=ms, iters=iters, warm_iters=warm_iters, timing=tm, diag=d,
+                dts=dts, clocks=ck, total_iters=d["total_iterations"] - d0)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- reference arm
+def reference_sample(q0, p, sor_iters=10):
+    """Time the reference's own C code (oracle/_ref) on one bounded sample of a
+    step: one hydro step (godunov_step_3d with gravity off) and `sor_iters`
+    iterations of gravity_solve_potential, each of which in the reference
+    re-evaluates the multipole boundary (gravity_solver_3d.c:712).  Returns
+    (t_hydro_s, t_iter_s)."""
+    from oracle.oracle import RefSim
+    r = RefSim(*p["shape"], lo=p["lo"], hi=p["hi"], G=p["G"], gamma=p["gamma"], cfl=p["cfl"],
+               bc=p["bc"], omega=1.5, max_iter=sor_iters, tol=0.0, grav_bc=1)
+    r.set_state(q0)
+    r.enable_gravity(False)
+    t = time.perf_counter()
+    r.step(1)
+    t_h = time.perf_counter() - t
+    rho = q0[0]
+    t = time.perf_counter()
+    r.gravity_solve(rho, potential_only=True)
+    t_it = (time.perf_counter() - t) / sor_iters
+    r.close()
+    return t_h, t_it
+
+
+REF_ITERS_FILE = os.path.join(ROOT, "hydrocode_astro1_b200", "data", "fp64_iterations.json")
+
+
+def reference_iterations(n):
+    """SOR iterations per warm step of the reference algorithm on this
+    workload.  The FP64 path is bit-identical to the reference, so its
+    iteration counts are the reference's; they are recorded by
+    `bench.py --variant fp64` into hydrocode_astro1_b200/data/."""
+    try:
+        with open(REF_ITERS_FILE) as f:
+            d = json.load(f)
+        return float(d[str(n)]["mean_warm_iterations"]), "recorded from the bit-identical FP64 path"
+    except Exception:
+        return None, "unknown"
+
+
+def main_reference(args):
+    world, rank, local, dist = dist_setup(args)
+    if rank != 0:
+        return 0
+    from oracle.oracle import have_reference
+    if not have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built"}))
+        return 0
+    q0, p = make_workload(args.n)
+    ncell = p["shape"][0] * p["shape"][1] * p["shape"][2]
+    I, src = reference_iterations(args.n)
+    if I is None:
+        I = 1000.0
+        src = "assumed 1000 (no recorded FP64 iteration count)"
+    for _ in range(args.warmup):
+        reference_sample(q0, p, sor_iters=2)
+    th, tit = [], []
+    for _ in range(args.steps):
+        a, b = reference_sample(q0, p, sor_iters=5)
+        th.append(a)
+        tit.append(b)
+    t_h, t_it = statistics.median(th), statistics.median(tit)
+    t_step = t_h + I * t_it
+    value = ncell / t_step / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"octant_explosion_{args.n}^3 (n=3 star, lmax 8, tol 1e-8)",
+                   "grid": list(p["shape"]), "parallelism": "serial reference (1 core)",
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"per step: 1 hydro step ({t_h:.2f} s) + 5 SOR iterations "
+                                   f"({t_it * 1e3:.0f} ms each) of the reference at {args.n}^3, "
+                                   f"extrapolated to {I:.0f} iterations/step ({src})"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def main_ours(args):
+    import numpy as np
+
+    import hydrocode_astro1_b200 as hc
+    world, rank, local, dist = dist_setup(args)
+    variant = "fp32" if args.variant == "best" else args.variant
+    q0, p = make_workload(args.n)
+    ncell = p["shape"][0] * p["shape"][1] * p["shape"][2]
+    clocks = Clocks(local)
+    r = run_variant(q0, p, variant, args.steps, args.warmup, local, dist, clocks)
+    ms = reduce_max(dist, r["ms"])
+    value = ncell * args.steps * world / (ms / 1e3) / 1e6
+    tm = r["timing"]
+    s = r["solver"]
+    fp64 = variant.startswith("fp64")
+
+    # roofline of the dominant kernel family (SOR sweeps)
+    interior = (p["shape"][0] - 2) * (p["shape"][1] - 2) * (p["shape"][2] - 2)
+    if fp64:
+        bytes_per_launch = interior * 24 / 2.0     # one colour sweep: half of 24 B/cell/iteration
+    else:
+        bytes_per_launch = interior * 12 / 2.0     # FP32 correction: e r/w + r read per iteration
+    sor_launches = max(tm["sor_launches"], 1)
+    sor_avg_ms = tm["sor_ms"] / sor_launches
+    pk, pk_kind = peaks()
+    achieved = bytes_per_launch / (sor_avg_ms / 1e3) / 1e9 if sor_avg_ms > 0 else 0.0
+    dominant = "sor_sweep"
+    shares = {k: tm[k] for k in ("hydro_ms", "bc_ms", "sor_ms", "residual_ms", "moments_ms", "unet_ms")}
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": pk, "unit": "GB/s",
+                "frac": achieved / pk, "peak_kind": pk_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "avg_launch_ms": sor_avg_ms, "launches": tm["sor_launches"]}
+    hydro_bytes = interior * (48 if not fp64 else 88)
+    hydro_avg = tm["hydro_ms"] / max(tm["hydro_launches"], 1)
+    hydro_roof = {"kernel": "hydro_interior", "achieved": hydro_bytes / (hydro_avg / 1e3) / 1e9 if hydro_avg else 0,
+                  "unit": "GB/s", "avg_launch_ms": hydro_avg,
+                  "algorithmic_bytes_per_launch": hydro_bytes}
+    hydro_roof["frac"] = hydro_roof["achieved"] / pk
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if fp64 else "f32 hydro / f64+f32 poisson",
+        "data": "synthetic",
+        "config": {"workload": f"octant_explosion_{args.n}^3 (n=3 star, lmax 8, tol 1e-8)",
+                   "grid": list(p["shape"]), "variant": variant,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (state >= 335 MB per buffer)"},
+        "sor_iterations_per_step": r["iters"],
+        "warmup_iterations": r["warm_iters"],
+        "time_ms": shares,
+        "roofline": roofline,
+        "roofline_hydro": hydro_roof,
+        "gpu_launches": tm["launches"],
+        "clocks": r["clocks"],
+    }
+
+    # the plain FP64 path on the same workload, for the FP32/FP64 speed-up
+    if not fp64 and not args.no_fp64_compare:
+        s.close()
+        r64 = run_variant(q0, p, "fp64", args.steps, args.warmup, local, dist, None)
+        ms64 = reduce_max(dist, r64["ms"])
+        v64 = ncell * args.steps * world / (ms64 / 1e3) / 1e6
+        line["fp64_plain"] = {"value": v64, "ms_per_step": ms64 / args.steps,
+                              "sor_iterations_per_step": r64["iters"],
+                              "speedup_of_value": value / v64}
+        r64["solver"].close()
+        s = hc.HydroSolver3D(p["shape"], **solver_kwargs(p, variant, local))
+        s.set_state(q0)
+        for _ in range(args.warmup):
+            s.step(1)
+
+    # end to end through the C ABI with host buffers (AoS State3D, pinned)
+    if not args.no_e2e:
+        from oracle.oracle import soa_to_aos  # layout helper only
+        U = hc.pin(soa_to_aos(s.state() if not fp64 else s.state()))
+        ne = min(args.steps, 3)
+        barrier(dist)
+        t = time.perf_counter()
+        for _ in range(ne):
+            s.step_host(U)
+        te = time.perf_counter() - t
+        te = reduce_max(dist, te)
+        hc.unpin(U)
+        line["e2e"] = {"value": ncell * ne * world / te / 1e6, "unit": UNIT,
+                       "h2d_bytes_per_step": int(U.nbytes), "d2h_bytes_per_step": int(U.nbytes),
+                       "steps": ne, "api": "hc_step_host (State3D host array in, out)"}
+    s.close()
+
+    # the reference C code on the host, bounded sample
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.oracle import have_reference
+        if have_reference():
+            th, tit = reference_sample(q0, p, sor_iters=5)
+            I = statistics.mean(r["iters"]) if fp64 else None
+            if I is None:
+                I, _src = reference_iterations(args.n)
+                if I is None and "fp64_plain" in line:
+                    I = statistics.mean(line["fp64_plain"]["sor_iterations_per_step"])
+            I = I or 1000.0
+            t_step = th + I * tit
+            line["cpu_baseline"] = {
+                "value": ncell / t_step / 1e6, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"1 hydro step ({th:.2f} s) + 5 SOR iterations ({tit * 1e3:.0f} ms each) "
+                          f"of the reference at {args.n}^3, extrapolated to {I:.0f} iterations/step"}
+        else:
+            line["cpu_baseline"] = None
+
+    if fp64 and rank == 0:
+        try:
+            os.makedirs(os.path.dirname(REF_ITERS_FILE), exist_ok=True)
+            d = {}
+            if os.path.exists(REF_ITERS_FILE):
+                d = json.load(open(REF_ITERS_FILE))
+            d[str(args.n)] = {"mean_warm_iterations": statistics.mean(r["iters"]),
+                              "per_step": r["iters"], "warmup": r["warm_iters"]}
+            json.dump(d, open(REF_ITERS_FILE, "w"), indent=1)
+        except Exception:
+            pass
+
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    a = parse()
+    sys.exit(main_reference(a) if a.impl == "reference" else main_ours(a))

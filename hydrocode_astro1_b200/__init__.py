@@ -1,0 +1,305 @@
+"""hydrocode_astro1_b200 -- B200 (sm_100a) hydro + self-gravity time step.
+
+Python mirror of the reference solver interface (hydro_solver_3d.h,
+gravity_solver_3d.h) over the C ABI of ``include/hydrocode_b200.h``, served by
+the in-tree shared library ``_lib/libhydrocode_b200.so``.  There is no CPU
+fallback: every compute call runs the CUDA kernels of that library, and
+constructing a solver fails loudly when the library or a GPU is missing.
+
+Conventions (the reference's): conserved state per cell rho, rhou, rhov,
+rhow, E; IDX3D ordering with k fastest (hydro_solver_3d.h:12); BCType 0
+periodic / 1 reflective / 2 outflow (input_deck.h:30-34); GravBCType 0
+periodic / 1 isolated / 2 dirichlet (gravity_solver_3d.h:10-14).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libhydrocode_b200.so")
+
+BC_PERIODIC, BC_REFLECTIVE, BC_OUTFLOW = 0, 1, 2
+GRAV_BC_PERIODIC, GRAV_BC_ISOLATED, GRAV_BC_DIRICHLET = 0, 1, 2
+FP64, FP32 = 0, 1
+MOMENTS_SEQUENTIAL, MOMENTS_TREE = 0, 1
+WARM_PREVIOUS, WARM_UNET = 0, 1
+
+HC_OK, HC_NOT_CONVERGED = 0, -1
+
+
+class HcError(RuntimeError):
+    pass
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double),
+        ("ymax", C.c_double), ("zmin", C.c_double), ("zmax", C.c_double),
+        ("gamma", C.c_double), ("cfl", C.c_double), ("G", C.c_double),
+        ("bc", C.c_int * 6), ("precision", C.c_int), ("moment_order", C.c_int),
+        ("grav_bc", C.c_int), ("lmax", C.c_int), ("omega", C.c_double),
+        ("tol", C.c_double), ("max_iter", C.c_int), ("sor_depth", C.c_int),
+        ("warm_start", C.c_int), ("device", C.c_int), ("gravity_only", C.c_int),
+    ]
+
+
+class Diag(C.Structure):
+    _fields_ = [
+        ("last_iterations", C.c_int), ("last_residual", C.c_double),
+        ("last_status", C.c_int), ("warm_start_used", C.c_int),
+        ("outer_cycles", C.c_int), ("dt", C.c_double), ("steps", C.c_longlong),
+        ("total_iterations", C.c_longlong), ("overshoot", C.c_int),
+    ]
+
+
+class Timing(C.Structure):
+    _fields_ = [
+        ("hydro_ms", C.c_double), ("bc_ms", C.c_double), ("sor_ms", C.c_double),
+        ("residual_ms", C.c_double), ("moments_ms", C.c_double), ("unet_ms", C.c_double),
+        ("hydro_launches", C.c_longlong), ("sor_launches", C.c_longlong),
+        ("launches", C.c_longlong),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+# name -> (restype, argtypes) of every C-ABI entry point in include/hydrocode_b200.h
+CAPI = {
+    "hc_config_default": (None, [C.POINTER(Config)]),
+    "hc_create": (C.c_void_p, [C.POINTER(Config)]),
+    "hc_destroy": (None, [C.c_void_p]),
+    "hc_ncells": (C.c_size_t, [C.c_void_p]),
+    "hc_set_state": (C.c_int, [C.c_void_p, _dp]),
+    "hc_get_state": (C.c_int, [C.c_void_p, _dp]),
+    "hc_set_state_soa": (C.c_int, [C.c_void_p, _dp]),
+    "hc_get_state_soa": (C.c_int, [C.c_void_p, _dp]),
+    "hc_step": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "hc_step_host": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "hc_gravity_solve": (C.c_int, [C.c_void_p, _dp, C.c_int]),
+    "hc_gravity_acceleration": (C.c_int, [C.c_void_p]),
+    "hc_set_gravity_params": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_double]),
+    "hc_set_gravity_bc": (C.c_int, [C.c_void_p, C.c_int]),
+    "hc_get_phi": (C.c_int, [C.c_void_p, _dp]),
+    "hc_set_phi": (C.c_int, [C.c_void_p, _dp]),
+    "hc_get_accel": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "hc_get_moments": (C.c_int, [C.c_void_p, _dp, C.c_int]),
+    "hc_residual_norm": (C.c_int, [C.c_void_p, _dp]),
+    "hc_get_diag": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
+    "hc_get_timing": (C.c_int, [C.c_void_p, C.POINTER(Timing), C.c_int]),
+    "hc_sync": (C.c_int, [C.c_void_p]),
+    "hc_timer_start": (C.c_int, [C.c_void_p]),
+    "hc_timer_stop": (C.c_int, [C.c_void_p, _dp]),
+    "hc_unet_param_count": (C.c_int, []),
+    "hc_unet_load": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint16), C.c_int]),
+    "hc_host_register": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "hc_host_unregister": (C.c_int, [C.c_void_p]),
+    "hc_last_error": (C.c_char_p, []),
+    "hc_device_count": (C.c_int, []),
+}
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HcError(f"{LIB_PATH} missing: build it with `make -C hydrocode_astro1_b200` "
+                          "or __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in CAPI.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error():
+    return lib().hc_last_error().decode(errors="replace")
+
+
+def device_count():
+    return lib().hc_device_count()
+
+
+def _check(rc, what):
+    if rc not in (HC_OK, HC_NOT_CONVERGED):
+        raise HcError(f"{what} failed ({rc}): {last_error()}")
+    return rc
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def default_config(**kw):
+    cfg = Config()
+    lib().hc_config_default(C.byref(cfg))
+    for k, v in kw.items():
+        if k == "bc":
+            for t in range(6):
+                cfg.bc[t] = int(v[t])
+        elif k in ("lo", "hi"):
+            names = ("xmin", "ymin", "zmin") if k == "lo" else ("xmax", "ymax", "zmax")
+            for nm, val in zip(names, v):
+                setattr(cfg, nm, float(val))
+        elif k == "shape":
+            cfg.nx, cfg.ny, cfg.nz = (int(x) for x in v)
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+class HydroSolver3D:
+    """One device solver: the reference's GodunovHLLC3D with its GravitySolver3D.
+
+    Mirrors solver3d_create / godunov_step_3d / gravity_solve and friends
+    (hydro_solver_3d.h:69-95, gravity_solver_3d.h:64-149).
+    """
+
+    def __init__(self, shape=None, **kw):
+        if shape is not None:
+            kw["shape"] = shape
+        self.cfg = default_config(**kw)
+        self.L = lib()
+        h = self.L.hc_create(C.byref(self.cfg))
+        if not h:
+            raise HcError(f"hc_create failed: {last_error()}")
+        self.h = h
+        self.shape = (self.cfg.nx, self.cfg.ny, self.cfg.nz)
+        self.n = self.cfg.nx * self.cfg.ny * self.cfg.nz
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # state -------------------------------------------------------------
+    def set_state(self, q):
+        """q: (5, nx, ny, nz) float64 conserved fields."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        assert q.shape == (5,) + self.shape
+        _check(self.L.hc_set_state_soa(self.h, _p(q)), "hc_set_state_soa")
+
+    def state(self):
+        q = np.empty((5,) + self.shape)
+        _check(self.L.hc_get_state_soa(self.h, _p(q)), "hc_get_state_soa")
+        return q
+
+    def set_state_aos(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.size == 5 * self.n
+        _check(self.L.hc_set_state(self.h, _p(U)), "hc_set_state")
+
+    def state_aos(self):
+        U = np.empty(5 * self.n)
+        _check(self.L.hc_get_state(self.h, _p(U)), "hc_get_state")
+        return U
+
+    # stepping ------------------------------------------------------------
+    def step(self, nsteps=1):
+        """godunov_step_3d nsteps times; returns the dt of each step."""
+        dts = np.zeros(max(nsteps, 1))
+        rc = _check(self.L.hc_step(self.h, nsteps, _p(dts)), "hc_step")
+        self.last_rc = rc
+        return dts[:nsteps]
+
+    def step_host(self, U):
+        """One step on a host State3D array (upload, step, download) in place."""
+        dt = C.c_double(0.0)
+        rc = _check(self.L.hc_step_host(self.h, _p(U), C.byref(dt)), "hc_step_host")
+        self.last_rc = rc
+        return dt.value
+
+    # gravity ---------------------------------------------------------------
+    def gravity_solve(self, rho=None, with_accel=True):
+        if rho is None:
+            rc = self.L.hc_gravity_solve(self.h, None, int(with_accel))
+        else:
+            rho = np.ascontiguousarray(rho, dtype=np.float64)
+            rc = self.L.hc_gravity_solve(self.h, _p(rho), int(with_accel))
+        return _check(rc, "hc_gravity_solve")
+
+    def set_gravity_params(self, omega, max_iter, tol):
+        _check(self.L.hc_set_gravity_params(self.h, omega, max_iter, tol), "hc_set_gravity_params")
+
+    def set_gravity_bc(self, bc):
+        _check(self.L.hc_set_gravity_bc(self.h, bc), "hc_set_gravity_bc")
+
+    def phi(self):
+        out = np.empty(self.shape)
+        _check(self.L.hc_get_phi(self.h, _p(out)), "hc_get_phi")
+        return out
+
+    def set_phi(self, phi):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        _check(self.L.hc_set_phi(self.h, _p(phi)), "hc_set_phi")
+
+    def accel(self):
+        gx, gy, gz = (np.empty(self.shape) for _ in range(3))
+        _check(self.L.hc_get_accel(self.h, _p(gx), _p(gy), _p(gz)), "hc_get_accel")
+        return gx, gy, gz
+
+    def gravity_acceleration(self):
+        _check(self.L.hc_gravity_acceleration(self.h), "hc_gravity_acceleration")
+
+    def moments(self):
+        cap = 4 + 13 * 13
+        out = np.zeros(cap)
+        _check(self.L.hc_get_moments(self.h, _p(out), cap), "hc_get_moments")
+        if self.cfg.lmax == 0:
+            return out[:13]
+        return out[:4 + (self.cfg.lmax + 1) ** 2]
+
+    def residual_norm(self):
+        v = C.c_double(0.0)
+        _check(self.L.hc_residual_norm(self.h, C.byref(v)), "hc_residual_norm")
+        return v.value
+
+    def diagnostics(self):
+        d = Diag()
+        _check(self.L.hc_get_diag(self.h, C.byref(d)), "hc_get_diag")
+        return {f: getattr(d, f) for f, _ in Diag._fields_}
+
+    def timing(self, reset=False):
+        t = Timing()
+        _check(self.L.hc_get_timing(self.h, C.byref(t), int(reset)), "hc_get_timing")
+        return {f: getattr(t, f) for f, _ in Timing._fields_}
+
+    def sync(self):
+        _check(self.L.hc_sync(self.h), "hc_sync")
+
+    def timer_start(self):
+        _check(self.L.hc_timer_start(self.h), "hc_timer_start")
+
+    def timer_stop(self):
+        v = C.c_double(0.0)
+        _check(self.L.hc_timer_stop(self.h, C.byref(v)), "hc_timer_stop")
+        return v.value
+
+
+def pin(array):
+    """Page-lock a numpy array's memory (cudaHostRegister); returns it."""
+    _check(lib().hc_host_register(array.ctypes.data, array.nbytes), "hc_host_register")
+    return array
+
+
+def unpin(array):
+    _check(lib().hc_host_unregister(array.ctypes.data), "hc_host_unregister")

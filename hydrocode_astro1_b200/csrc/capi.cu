@@ -1,0 +1,1054 @@
+// capi.cu -- the C ABI (include/hydrocode_b200.h): device context, the step
+// and Poisson-solve orchestration on one CUDA stream.
+//
+// Memory: one context owns its buffers (cudaMalloc at create, freed at
+// destroy).  State lives in structure-of-arrays form, double-buffered so a
+// step reads step-n values and writes step n+1 (the reference achieves the
+// same with its separate flux arrays).  The host is crossed only for the
+// per-step dt, the SOR stop flag every few dozen iterations, and explicit
+// state/potential transfers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "hc_internal.cuh"
+
+using namespace hc;
+
+// ---------------------------------------------------------------- errors
+static thread_local char g_err[512] = "";
+
+static int set_err(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return set_err(HC_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,        \
+                           cudaGetErrorString(e_));                                      \
+    } while (0)
+
+extern "C" const char *hc_last_error(void) { return g_err; }
+
+extern "C" int hc_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+// ---------------------------------------------------------------- context
+struct EvPair {
+    cudaEvent_t a, b;
+    int fam;
+};
+
+enum { FAM_HYDRO = 0, FAM_BC, FAM_SOR, FAM_RES, FAM_MOM, FAM_UNET, FAM_N };
+
+struct hc_ctx {
+    hc_config cfg;
+    Geom g;
+    int dev;
+    cudaStream_t s;
+    int gravity;                 // self-gravity enabled
+    // state
+    double *q64[2][5];
+    float *q32[2][5];
+    int cur;
+    int parity;
+    int cfl_valid;
+    // gravity
+    double *phi, *phig, *rho_ext, *phi2;
+    float *e32, *r32, *e32b;     // mixed precision correction (ping-pong) / residual
+    double *gx, *gy, *gz;
+    double *res;
+    int res_cap;
+    double *scratch;
+    long long scratch_len;
+    double *mom;
+    // scalars
+    DevScalars *sc;
+    DevScalars *hsc;             // pinned mirror
+    double *stage;               // AoS staging buffer on the device
+    double *hdt;                 // pinned dt ring
+    int hdt_cap;
+    double *hslots;              // pinned copy of recent SOR update norms
+    // diagnostics + timing
+    hc_diag diag;
+    double fam_ms[FAM_N];
+    long long launches, hydro_launches, sor_launches;
+    std::vector<EvPair> pend;
+    std::vector<cudaEvent_t> evpool;
+    // learned warm start
+    void *unet;
+    // user timer
+    cudaEvent_t t0, t1;
+    int timer_on;
+};
+
+static cudaEvent_t ev_get(hc_ctx *c)
+{
+    if (!c->evpool.empty()) {
+        cudaEvent_t e = c->evpool.back();
+        c->evpool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+struct FamTimer {
+    hc_ctx *c;
+    EvPair p;
+    FamTimer(hc_ctx *c_, int fam) : c(c_)
+    {
+        p.a = ev_get(c);
+        p.b = ev_get(c);
+        p.fam = fam;
+        if (p.a) cudaEventRecord(p.a, c->s);
+    }
+    ~FamTimer()
+    {
+        if (p.b) cudaEventRecord(p.b, c->s);
+        if (p.a && p.b) c->pend.push_back(p);
+    }
+};
+
+static void resolve_timers(hc_ctx *c)
+{
+    for (auto &p : c->pend) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) c->fam_ms[p.fam] += ms;
+        c->evpool.push_back(p.a);
+        c->evpool.push_back(p.b);
+    }
+    c->pend.clear();
+}
+
+static int sync_ctx(hc_ctx *c)
+{
+    CK(cudaStreamSynchronize(c->s));
+    resolve_timers(c);
+    return HC_OK;
+}
+
+extern "C" void hc_config_default(hc_config *cfg)
+{
+    memset(cfg, 0, sizeof *cfg);
+    cfg->nx = cfg->ny = cfg->nz = 64;
+    cfg->xmin = cfg->ymin = cfg->zmin = 0.0;
+    cfg->xmax = cfg->ymax = cfg->zmax = 1.0;
+    cfg->gamma = 5.0 / 3.0;   // hydro_solver_3d.c:61
+    cfg->cfl = 0.4;           // hydro_solver_3d.c:59
+    cfg->G = 0.0;
+    for (int t = 0; t < 6; t++) cfg->bc[t] = 2;
+    cfg->precision = HC_FP64;
+    cfg->moment_order = HC_MOMENTS_SEQUENTIAL;
+    cfg->grav_bc = 1;          // ISOLATED, hydro_solver_3d.c:78
+    cfg->lmax = 0;
+    cfg->omega = 1.5;          // gravity_solver_3d.c:78-80
+    cfg->max_iter = 10000;
+    cfg->tol = 1.0e-6;
+    cfg->sor_depth = 0;
+    cfg->warm_start = HC_WARM_PREVIOUS;
+    cfg->device = 0;
+}
+
+static void free_ctx(hc_ctx *c)
+{
+    if (!c) return;
+    if (c->dev >= 0) cudaSetDevice(c->dev);
+    for (int b = 0; b < 2; b++)
+        for (int v = 0; v < 5; v++) {
+            if (c->q64[b][v] && v == 0) cudaFree(c->q64[b][0]);
+            if (c->q32[b][v] && v == 0) cudaFree(c->q32[b][0]);
+        }
+    cudaFree(c->phi); cudaFree(c->phig); cudaFree(c->rho_ext); cudaFree(c->phi2);
+    cudaFree(c->e32); cudaFree(c->r32); cudaFree(c->e32b);
+    cudaFree(c->gx); cudaFree(c->gy); cudaFree(c->gz);
+    cudaFree(c->res); cudaFree(c->scratch); cudaFree(c->mom);
+    cudaFree(c->sc); cudaFree(c->stage);
+    if (c->hsc) cudaFreeHost(c->hsc);
+    if (c->hdt) cudaFreeHost(c->hdt);
+    if (c->hslots) cudaFreeHost(c->hslots);
+    resolve_timers(c);
+    for (auto e : c->evpool) cudaEventDestroy(e);
+    if (c->t0) cudaEventDestroy(c->t0);
+    if (c->t1) cudaEventDestroy(c->t1);
+    if (c->s) cudaStreamDestroy(c->s);
+    extern void hc_unet_free(void *);
+    if (c->unet) hc_unet_free(c->unet);
+    delete c;
+}
+
+static int dmalloc(void **p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_err(HC_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return HC_OK;
+}
+
+static int ensure_res(hc_ctx *c, int max_iter)
+{
+    int need = std::max(max_iter, 1) + 16;   // slack for blocked passes
+    if (c->res && c->res_cap >= need) return HC_OK;
+    cudaFree(c->res);
+    c->res = nullptr;
+    int cap = std::max(need, 1024);
+    int rc = dmalloc((void **)&c->res, sizeof(double) * cap);
+    if (rc) return rc;
+    c->res_cap = cap;
+    return HC_OK;
+}
+
+extern "C" hc_ctx *hc_create(const hc_config *cfg)
+{
+    if (!cfg) { set_err(HC_ERR_ARG, "null config"); return nullptr; }
+    const hc_config &k = *cfg;
+    if (k.nx < 3 || k.ny < 3 || (k.nz < 3 && !(k.gravity_only && k.nz == 1))) {
+        set_err(HC_ERR_ARG, "grid %dx%dx%d: every dimension needs at least 3 cells "
+                "(nz == 1 only for a gravity-only context)", k.nx, k.ny, k.nz);
+        return nullptr;
+    }
+    if (k.gravity_only && !(k.G > 0.0)) {
+        set_err(HC_ERR_ARG, "gravity-only context needs G > 0");
+        return nullptr;
+    }
+    if (k.precision != HC_FP64 && k.precision != HC_FP32) {
+        set_err(HC_ERR_ARG, "unknown precision %d", k.precision);
+        return nullptr;
+    }
+    if (k.lmax < 0 || k.lmax > 12) {
+        set_err(HC_ERR_ARG, "lmax %d outside 0..12", k.lmax);
+        return nullptr;
+    }
+    if (!(k.xmax > k.xmin) || !(k.ymax > k.ymin) || !(k.zmax > k.zmin)) {
+        set_err(HC_ERR_ARG, "empty domain");
+        return nullptr;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        set_err(HC_ERR_CUDA, "no CUDA device available");
+        return nullptr;
+    }
+    if (k.device < 0 || k.device >= ndev) {
+        set_err(HC_ERR_ARG, "device %d not present (%d devices)", k.device, ndev);
+        return nullptr;
+    }
+    const char *fail = getenv("HC_FAIL_ALLOC");   // host-side fault injection for tests
+    if (fail && atoi(fail) != 0) {
+        set_err(HC_ERR_NOMEM, "allocation failure injected by HC_FAIL_ALLOC");
+        return nullptr;
+    }
+    hc_ctx *c = new hc_ctx();
+    memset(c->q64, 0, sizeof c->q64);
+    memset(c->q32, 0, sizeof c->q32);
+    c->cfg = k;
+    c->dev = k.device;
+    if (cudaSetDevice(c->dev) != cudaSuccess) { set_err(HC_ERR_CUDA, "cudaSetDevice"); delete c; return nullptr; }
+    Geom &g = c->g;
+    g.nx = k.nx; g.ny = k.ny; g.nz = k.nz;
+    g.n = (long long)k.nx * k.ny * k.nz;
+    g.xmin = k.xmin; g.xmax = k.xmax; g.ymin = k.ymin; g.ymax = k.ymax; g.zmin = k.zmin; g.zmax = k.zmax;
+    g.dx = (k.xmax - k.xmin) / k.nx;
+    g.dy = (k.ymax - k.ymin) / k.ny;
+    g.dz = (k.zmax - k.zmin) / k.nz;
+    c->gravity = k.G > 0.0;
+    const size_t n = (size_t)g.n;
+    int rc = HC_OK;
+    if (cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking) != cudaSuccess) {
+        set_err(HC_ERR_CUDA, "stream create");
+        free_ctx(c);
+        return nullptr;
+    }
+    for (int b = 0; b < 2 && !rc && !k.gravity_only; b++) {
+        if (k.precision == HC_FP64) {
+            double *base = nullptr;
+            rc = dmalloc((void **)&base, 5 * n * sizeof(double));
+            for (int v = 0; v < 5 && !rc; v++) c->q64[b][v] = base + v * n;
+        } else {
+            float *base = nullptr;
+            rc = dmalloc((void **)&base, 5 * n * sizeof(float));
+            for (int v = 0; v < 5 && !rc; v++) c->q32[b][v] = base + v * n;
+        }
+    }
+    if (!rc) rc = dmalloc((void **)&c->sc, sizeof(DevScalars));
+    if (!rc && c->gravity) {
+        rc = dmalloc((void **)&c->phi, n * sizeof(double));
+        if (!rc) rc = dmalloc((void **)&c->phig, n * sizeof(double));
+        if (!rc) rc = ensure_res(c, k.max_iter);
+        c->scratch_len = 64 * 1024;   // tree partials (592x9) and lmax partials (296x169)
+        if (!rc) rc = dmalloc((void **)&c->scratch, c->scratch_len * sizeof(double));
+        if (!rc) rc = dmalloc((void **)&c->mom, 4 * 1024 * sizeof(double));
+        if (!rc && k.precision == HC_FP32) {
+            rc = dmalloc((void **)&c->e32, n * sizeof(float));
+            if (!rc) rc = dmalloc((void **)&c->r32, n * sizeof(float));
+            if (!rc) rc = dmalloc((void **)&c->e32b, n * sizeof(float));
+        }
+    }
+    if (!rc && cudaMallocHost((void **)&c->hsc, sizeof(DevScalars)) != cudaSuccess)
+        rc = set_err(HC_ERR_NOMEM, "pinned scalars");
+    if (rc) { free_ctx(c); return nullptr; }
+    // zero state and potential (calloc in the reference, gravity_solver_3d.c:87)
+    cudaMemsetAsync(c->sc, 0, sizeof(DevScalars), c->s);
+    for (int b = 0; b < 2; b++) {
+        if (c->q64[b][0]) cudaMemsetAsync(c->q64[b][0], 0, 5 * n * sizeof(double), c->s);
+        if (c->q32[b][0]) cudaMemsetAsync(c->q32[b][0], 0, 5 * n * sizeof(float), c->s);
+    }
+    if (c->e32b) {
+        cudaMemsetAsync(c->e32, 0, n * sizeof(float), c->s);
+        cudaMemsetAsync(c->e32b, 0, n * sizeof(float), c->s);
+    }
+    if (c->phi) {
+        cudaMemsetAsync(c->phi, 0, n * sizeof(double), c->s);
+        cudaMemsetAsync(c->phig, 0, n * sizeof(double), c->s);
+    }
+    if (cudaStreamSynchronize(c->s) != cudaSuccess) {
+        set_err(HC_ERR_CUDA, "init memset");
+        free_ctx(c);
+        return nullptr;
+    }
+    c->cur = 0;
+    c->parity = 0;
+    c->cfl_valid = 0;
+    return c;
+}
+
+extern "C" void hc_destroy(hc_ctx *c) { free_ctx(c); }
+
+extern "C" size_t hc_ncells(const hc_ctx *c) { return c ? (size_t)c->g.n : 0; }
+
+// ---------------------------------------------------------------- state I/O
+static int ensure_stage(hc_ctx *c)
+{
+    if (c->stage) return HC_OK;
+    return dmalloc((void **)&c->stage, 5 * (size_t)c->g.n * sizeof(double));
+}
+
+static int upload_soa64(hc_ctx *c, const double *q)
+{
+    const size_t n = (size_t)c->g.n;
+    if (c->cfg.precision == HC_FP64) {
+        for (int v = 0; v < 5; v++)
+            CK(cudaMemcpyAsync(c->q64[c->cur][v], q + v * n, n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+    } else {
+        int rc = ensure_stage(c);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(c->stage, q, 5 * n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        double *src[5];
+        for (int v = 0; v < 5; v++) src[v] = c->stage + v * n;
+        CK(fp32_from_fp64(src, c->q32[c->cur], c->g.n, c->s));
+    }
+    c->cfl_valid = 0;
+    return HC_OK;
+}
+
+extern "C" int hc_set_state(hc_ctx *c, const double *U)
+{
+    if (!c || !U) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    const size_t n = (size_t)c->g.n;
+    CK(cudaMemcpyAsync(c->stage, U, 5 * n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+    if (c->cfg.precision == HC_FP64) CK(fp64_aos_to_soa(c->stage, c->q64[c->cur], c->g.n, c->s));
+    else CK(fp32_from_aos64(c->stage, c->q32[c->cur], c->g.n, c->s));
+    c->cfl_valid = 0;
+    c->launches += 1;
+    return sync_ctx(c);
+}
+
+extern "C" int hc_get_state(hc_ctx *c, double *U)
+{
+    if (!c || !U) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    const size_t n = (size_t)c->g.n;
+    if (c->cfg.precision == HC_FP64) CK(fp64_soa_to_aos(c->q64[c->cur], c->stage, c->g.n, c->s));
+    else CK(fp32_to_aos64(c->q32[c->cur], c->stage, c->g.n, c->s));
+    CK(cudaMemcpyAsync(U, c->stage, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_set_state_soa(hc_ctx *c, const double *q)
+{
+    if (!c || !q) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = upload_soa64(c, q);
+    if (rc) return rc;
+    return sync_ctx(c);
+}
+
+extern "C" int hc_get_state_soa(hc_ctx *c, double *q)
+{
+    if (!c || !q) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    const size_t n = (size_t)c->g.n;
+    if (c->cfg.precision == HC_FP64) {
+        for (int v = 0; v < 5; v++)
+            CK(cudaMemcpyAsync(q + v * n, c->q64[c->cur][v], n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    } else {
+        int rc = ensure_stage(c);
+        if (rc) return rc;
+        double *dst[5];
+        for (int v = 0; v < 5; v++) dst[v] = c->stage + v * n;
+        CK(fp32_to_fp64(c->q32[c->cur], dst, c->g.n, c->s));
+        CK(cudaMemcpyAsync(q, c->stage, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    }
+    return sync_ctx(c);
+}
+
+// ---------------------------------------------------------------- gravity
+static GravArgs grav_args(hc_ctx *c, const double *rho, const float *rho32)
+{
+    GravArgs a;
+    memset(&a, 0, sizeof a);
+    a.g = c->g;
+    a.G = c->cfg.G;
+    a.omega = c->cfg.omega;
+    a.tol = c->cfg.tol;
+    a.max_iter = c->cfg.max_iter;
+    a.grav_bc = c->cfg.grav_bc;
+    a.lmax = c->cfg.lmax;
+    a.moment_order = c->cfg.moment_order;
+    a.phi = c->phi;
+    a.rho = rho;
+    a.rho32 = rho32;
+    a.res = c->res;
+    a.sc = c->sc;
+    a.scratch = c->scratch;
+    a.scratch_len = c->scratch_len;
+    a.mom = c->mom;
+    a.gx = c->gx; a.gy = c->gy; a.gz = c->gz;
+    return a;
+}
+
+// Multipole moments + boundary values of the current density.
+static int grav_boundary_values(hc_ctx *c, const GravArgs &a)
+{
+    if (a.grav_bc == 0) {
+        CK(grav_boundary_periodic(a, c->s));
+        c->launches += 3;
+        return HC_OK;
+    }
+    if (a.grav_bc != 1) return HC_OK;   // DIRICHLET keeps the current values
+    FamTimer t(c, FAM_MOM);
+    if (a.lmax == 0) {
+        CK(grav_boundary_ref(a, c->s));
+        c->launches += 1;
+    } else {
+        CK(grav_boundary_lmax(a, c->s));
+        c->launches += 1;
+    }
+    return HC_OK;
+}
+
+static int grav_moments(hc_ctx *c, const GravArgs &a)
+{
+    if (a.grav_bc != 1) return HC_OK;
+    FamTimer t(c, FAM_MOM);
+    if (a.lmax == 0) {
+        if (a.moment_order == HC_MOMENTS_SEQUENTIAL && a.rho) {
+            CK(grav_moments_sequential(a, c->s));
+            c->launches += 1;
+        } else {
+            CK(grav_moments_tree(a, c->s));
+            c->launches += 4;
+        }
+    } else {
+        CK(grav_moments_lmax(a, c->s));
+        c->launches += 4;
+    }
+    return HC_OK;
+}
+
+// Red-black SOR to tolerance, FP64 (gravity_solve_potential,
+// gravity_solver_3d.c:510-747).  Returns 0 / -1 like the reference, or a
+// negative HC_ERR_* code.
+static int sor_fp64(hc_ctx *c, const double *rho)
+{
+    GravArgs a = grav_args(c, rho, nullptr);
+    int rc = ensure_res(c, a.max_iter);
+    if (rc) return rc;
+    a.res = c->res;
+    CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));    // done, last_iter
+    CK(grav_reset_slots(a, 0, std::max(a.max_iter, 1), c->s));
+    rc = grav_moments(c, a);
+    if (rc) return rc;
+    if (a.max_iter <= 0) {
+        c->diag.last_iterations = 0;
+        c->diag.last_residual = 0.0;
+        return -1;
+    }
+    // sor_depth -1: one kernel per colour, in place (the reference's sweeps);
+    // otherwise one wavefront pass per iteration, out of place between
+    // phi (buf 0) and phi2 (buf 1): iteration t reads buf[t%2], writes buf[(t+1)%2]
+    const bool wave = c->cfg.sor_depth >= 0 && c->g.nz >= 3;
+    double *buf[2] = { c->phi, c->phi2 };
+    if (wave) {
+        if (!c->phi2) {
+            rc = dmalloc((void **)&c->phi2, (size_t)c->g.n * sizeof(double));
+            if (rc) return rc;
+            buf[1] = c->phi2;
+        }
+        // both buffers carry the current boundary cells
+        CK(cudaMemcpyAsync(c->phi2, c->phi, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+    }
+    auto one_iter = [&](int q) -> int {
+        if (wave) {
+            CK(grav_sor_pass64(a, buf[q & 1], buf[(q + 1) & 1], q, c->s));
+            c->launches += 1;
+            c->sor_launches += 1;
+        } else {
+            CK(grav_sor_color(a, 0, q, c->s));
+            CK(grav_sor_color(a, 1, q, c->s));
+            c->launches += 2;
+            c->sor_launches += 2;
+        }
+        return HC_OK;
+    };
+    {
+        FamTimer t(c, FAM_SOR);
+        rc = one_iter(0);
+        if (rc) return rc;
+    }
+    // the first iteration swept with the previous boundary; now the new one
+    if (wave) {
+        GravArgs b = a;
+        b.phi = buf[1];
+        rc = grav_boundary_values(c, b);
+        if (rc) return rc;
+    }
+    rc = grav_boundary_values(c, a);
+    if (rc) return rc;
+    int it = 1, done = 0, last = 0;
+    int batch = 16;
+    while (true) {
+        int end = std::min(a.max_iter, it + batch);
+        {
+            FamTimer t(c, FAM_SOR);
+            for (int q = it; q < end; q++) {
+                rc = one_iter(q);
+                if (rc) return rc;
+            }
+            CK(grav_check(a, end, c->s));
+        }
+        c->launches += 1;
+        CK(cudaMemcpyAsync(&c->hsc->done, &c->sc->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+        rc = sync_ctx(c);
+        if (rc) return rc;
+        done = c->hsc->done;
+        last = c->hsc->last_iter;
+        if (done || end >= a.max_iter) break;
+        it = end;
+        batch = std::min(batch * 2, 256);
+    }
+    int used = done ? last : a.max_iter;
+    if (wave && (used & 1)) std::swap(c->phi, c->phi2);   // result in buf[used % 2]
+    double rv = 0.0;
+    CK(cudaMemcpy(&rv, c->res + (used - 1), sizeof(double), cudaMemcpyDeviceToHost));
+    c->diag.last_iterations = used;
+    c->diag.last_residual = rv;
+    c->diag.total_iterations += used;
+    return done ? 0 : -1;
+}
+
+// Mixed-precision Poisson solve: FP64 residual of the full potential, FP32
+// red-black SOR on the correction, FP64 update; repeated until the FP64
+// update norm max|delta| is below tol.  Iteration budget: max_iter inner
+// sweeps in total.
+int hc_sor_mixed(hc_ctx *c, const float *rho32)
+{
+    GravArgs a = grav_args(c, nullptr, rho32);
+    int rc = ensure_res(c, a.max_iter);
+    if (rc) return rc;
+    a.res = c->res;
+    rc = grav_moments(c, a);
+    if (rc) return rc;
+    rc = grav_boundary_values(c, a);
+    if (rc) return rc;
+    int total = 0, cycles = 0, status = -1;
+    double dmax = 0.0;
+    while (true) {
+        {
+            FamTimer t(c, FAM_RES);
+            CK(cudaMemsetAsync(&c->sc->resnorm, 0, sizeof(double), c->s));
+            CK(mixed_residual(a, c->r32, c->e32, c->s));
+            c->launches++;
+        }
+        CK(cudaMemcpyAsync(&c->hsc->resnorm, &c->sc->resnorm, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+        rc = sync_ctx(c);
+        if (rc) return rc;
+        dmax = c->hsc->resnorm;
+        cycles++;
+        if (!std::isfinite(dmax)) return set_err(HC_ERR_NUMERIC, "non-finite Poisson residual");
+        if (dmax < a.tol) { status = 0; break; }
+        if (total >= a.max_iter) break;
+        // one cycle reduces the residual 1e4-fold at most: FP32 resolves the
+        // correction e to ~1e-7 |e|, and |e| can exceed max|delta| by the
+        // grid's condition number on a cold start
+        const double thresh = std::max(0.5 * a.tol, 1.0e-4 * dmax);
+        const int budget = a.max_iter - total;
+        CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));
+        CK(grav_reset_slots(a, 0, budget + 8, c->s));
+        // depth: FP32 iterations per HBM pass (temporal blocking); -1 selects
+        // one in-place kernel per colour
+        const int depth = c->cfg.sor_depth == 0 ? 4 : c->cfg.sor_depth;
+        float *eb[2] = { c->e32, c->e32b };
+        int it = 0, done = 0, last = 0, batch = 16, processed = 0, best_it = 0;
+        double best = 1e300;
+        if (!c->hslots && cudaMallocHost((void **)&c->hslots, 512 * sizeof(double)) != cudaSuccess)
+            return set_err(HC_ERR_NOMEM, "pinned slot buffer");
+        while (true) {
+            int end = std::min(budget, it + batch);
+            {
+                FamTimer t(c, FAM_SOR);
+                if (depth < 0) {
+                    for (int q = it; q < end; q++) {
+                        CK(mixed_sor32(a, c->e32, c->r32, 0, q, thresh, c->s));
+                        CK(mixed_sor32(a, c->e32, c->r32, 1, q, thresh, c->s));
+                    }
+                    c->launches += 2 * (end - it);
+                    c->sor_launches += 2 * (end - it);
+                } else {
+                    // passes start at multiples of depth; the last may overrun the
+                    // budget by < depth iterations (slots are sized for it)
+                    for (int q = it; q < end; q += depth) {
+                        CK(mixed_sor32_pass(a, eb[(q / depth) & 1], eb[((q / depth) + 1) & 1], c->r32, q,
+                                            depth, thresh, c->s));
+                        c->launches += 1;
+                        c->sor_launches += 1;
+                    }
+                    end = it + ((end - it + depth - 1) / depth) * depth;
+                }
+                CK(mixed_check(a, end, thresh, c->s));
+                c->launches += 1;
+            }
+            processed = end;
+            CK(cudaMemcpyAsync(&c->hsc->done, &c->sc->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+            const int nb = std::min(end - it, 512);
+            CK(cudaMemcpyAsync(c->hslots, c->res + (end - nb), nb * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+            rc = sync_ctx(c);
+            if (rc) return rc;
+            done = c->hsc->done;
+            last = c->hsc->last_iter;
+            if (done || end >= budget) break;
+            // stagnation guard: FP32 round-off floor reached before thresh
+            for (int q = 0; q < nb; q++) {
+                double v = c->hslots[q];
+                if (v > 0.0 && v < 0.995 * best) { best = v; best_it = end - nb + q; }
+            }
+            if (end - best_it > 2048) break;
+            it = end;
+            batch = std::min(batch * 2, 256);
+        }
+        const int used = done ? last : processed;
+        total += used;
+        // the correction is in eb[passes % 2] for the blocked sweeps
+        const float *efinal = (depth < 0) ? c->e32 : eb[(used / depth) & 1];
+        {
+            FamTimer t(c, FAM_RES);
+            CK(mixed_update(a, efinal, c->s));
+            c->launches++;
+        }
+    }
+    c->diag.last_iterations = total;
+    c->diag.last_residual = dmax;
+    c->diag.outer_cycles = cycles;
+    c->diag.total_iterations += total;
+    return status;
+}
+
+static int gravity_solve_dev(hc_ctx *c, const double *rho64, const float *rho32)
+{
+    int st;
+    if (c->cfg.precision == HC_FP64 || rho64) {
+        st = sor_fp64(c, rho64);
+    } else {
+        st = hc_sor_mixed(c, rho32);
+    }
+    if (st < -1) return st;
+    c->diag.last_status = st;
+    if (st == 0) CK(cudaMemcpyAsync(c->phig, c->phi, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+    else
+        fprintf(stderr, "Warning: Gravity solver did not converge in %d iterations.\n"
+                        "         Final residual: %.3e (tolerance: %.3e)\n",
+                c->diag.last_iterations, c->diag.last_residual, c->cfg.tol);
+    return st;
+}
+
+extern "C" int hc_gravity_solve(hc_ctx *c, const double *rho, int with_accel)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled (G <= 0)");
+    CK(cudaSetDevice(c->dev));
+    const size_t n = (size_t)c->g.n;
+    int st;
+    if (rho) {
+        if (!c->rho_ext) {
+            int rc = dmalloc((void **)&c->rho_ext, n * sizeof(double));
+            if (rc) return rc;
+        }
+        CK(cudaMemcpyAsync(c->rho_ext, rho, n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+        st = gravity_solve_dev(c, c->rho_ext, nullptr);
+    } else if (c->cfg.precision == HC_FP64) {
+        st = gravity_solve_dev(c, c->q64[c->cur][0], nullptr);
+    } else {
+        st = gravity_solve_dev(c, nullptr, c->q32[c->cur][0]);
+    }
+    if (st < -1) return st;
+    (void)with_accel;   // g is formed from the converged potential on demand
+    int rc = sync_ctx(c);
+    if (rc) return rc;
+    return st == 0 ? HC_OK : HC_NOT_CONVERGED;
+}
+
+static int ensure_accel(hc_ctx *c)
+{
+    const size_t n = (size_t)c->g.n;
+    int rc = HC_OK;
+    if (!c->gx) rc = dmalloc((void **)&c->gx, n * sizeof(double));
+    if (!rc && !c->gy) rc = dmalloc((void **)&c->gy, n * sizeof(double));
+    if (!rc && !c->gz) rc = dmalloc((void **)&c->gz, n * sizeof(double));
+    return rc;
+}
+
+extern "C" int hc_gravity_acceleration(hc_ctx *c)
+{
+    // gravity_compute_acceleration on the current potential: it becomes the
+    // potential that the step's source term uses.
+    if (!c || !c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(c->phig, c->phi, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_get_accel(hc_ctx *c, double *gx, double *gy, double *gz)
+{
+    if (!c || !gx || !gy || !gz) return set_err(HC_ERR_ARG, "null argument");
+    if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
+    CK(cudaSetDevice(c->dev));
+    int rc = ensure_accel(c);
+    if (rc) return rc;
+    GravArgs a = grav_args(c, nullptr, nullptr);
+    a.phi = c->phig;
+    CK(grav_accel(a, c->s));
+    const size_t n = (size_t)c->g.n;
+    CK(cudaMemcpyAsync(gx, c->gx, n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaMemcpyAsync(gy, c->gy, n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    CK(cudaMemcpyAsync(gz, c->gz, n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_get_phi(hc_ctx *c, double *phi)
+{
+    if (!c || !phi) return set_err(HC_ERR_ARG, "null argument");
+    if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(phi, c->phi, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_set_phi(hc_ctx *c, const double *phi)
+{
+    if (!c || !phi) return set_err(HC_ERR_ARG, "null argument");
+    if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(c->phi, phi, (size_t)c->g.n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_get_moments(hc_ctx *c, double *mom, int cap)
+{
+    if (!c || !mom || cap < 13) return set_err(HC_ERR_ARG, "bad argument");
+    if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
+    CK(cudaSetDevice(c->dev));
+    if (c->cfg.lmax == 0) {
+        CK(cudaMemcpyAsync(c->hsc->moments, c->sc->moments, sizeof(double) * 13, cudaMemcpyDeviceToHost, c->s));
+        int rc = sync_ctx(c);
+        if (rc) return rc;
+        memcpy(mom, c->hsc->moments, sizeof(double) * 13);
+        return HC_OK;
+    }
+    int nc = 4 + lmax_ncoef(c->cfg.lmax);
+    if (cap < nc) return set_err(HC_ERR_ARG, "need %d doubles", nc);
+    CK(cudaMemcpyAsync(mom, c->mom, sizeof(double) * nc, cudaMemcpyDeviceToHost, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_set_gravity_params(hc_ctx *c, double omega, int max_iter, double tol)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    c->cfg.omega = omega;
+    c->cfg.max_iter = max_iter;
+    c->cfg.tol = tol;
+    if (c->gravity) {
+        CK(cudaSetDevice(c->dev));
+        return ensure_res(c, max_iter);
+    }
+    return HC_OK;
+}
+
+extern "C" int hc_set_gravity_bc(hc_ctx *c, int bc)
+{
+    if (!c || bc < 0 || bc > 2) return set_err(HC_ERR_ARG, "bad gravity bc");
+    c->cfg.grav_bc = bc;
+    return HC_OK;
+}
+
+extern "C" int hc_residual_norm(hc_ctx *c, double *out)
+{
+    if (!c || !out) return set_err(HC_ERR_ARG, "null argument");
+    if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
+    CK(cudaSetDevice(c->dev));
+    GravArgs a = c->cfg.precision == HC_FP64 ? grav_args(c, c->q64[c->cur][0], nullptr)
+                                             : grav_args(c, nullptr, c->q32[c->cur][0]);
+    CK(cudaMemsetAsync(&c->sc->resnorm, 0, sizeof(double), c->s));
+    CK(grav_residual_norm(a, c->phi, c->s));
+    CK(cudaMemcpyAsync(&c->hsc->resnorm, &c->sc->resnorm, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    int rc = sync_ctx(c);
+    if (rc) return rc;
+    *out = c->hsc->resnorm;
+    return HC_OK;
+}
+
+// ---------------------------------------------------------------- step
+static HydroArgs hydro_args(hc_ctx *c)
+{
+    HydroArgs a;
+    memset(&a, 0, sizeof a);
+    a.g = c->g;
+    a.gamma = c->cfg.gamma;
+    a.cfl = c->cfg.cfl;
+    for (int t = 0; t < 6; t++) a.bc[t] = c->cfg.bc[t];
+    a.gravity = c->gravity;
+    const int nxt = c->cur ^ 1;
+    for (int v = 0; v < 5; v++) {
+        if (c->cfg.precision == HC_FP64) {
+            a.qin[v] = c->q64[c->cur][v];
+            a.qout[v] = c->q64[nxt][v];
+        } else {
+            a.qin[v] = c->q32[c->cur][v];
+            a.qout[v] = c->q32[nxt][v];
+        }
+    }
+    a.phig = c->phig;
+    a.sc = c->sc;
+    a.step_parity = c->parity;
+    return a;
+}
+
+static int interior_chunks(const hc_ctx *c)
+{
+    long long tiles = (long long)((c->g.nz + 31) / 32) * ((c->g.ny + 7) / 8);
+    long long want = 148LL * 2 * 4;   // ~4 waves of 2 resident blocks per SM
+    long long ch = (want + tiles - 1) / tiles;
+    ch = std::max(1LL, std::min(ch, (long long)(c->g.nx - 2)));
+    // keep at least 8 planes per chunk so the prologue plane stays cheap
+    ch = std::min(ch, std::max(1LL, (long long)(c->g.nx - 2) / 8));
+    return (int)ch;
+}
+
+// One godunov step on the device state (no host synchronisation).
+static int step_once(hc_ctx *c, int *grav_status)
+{
+    if (c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    const bool f64 = c->cfg.precision == HC_FP64;
+    if (!c->cfl_valid) {
+        HydroArgs a = hydro_args(c);
+        FamTimer t(c, FAM_BC);
+        CK(f64 ? fp64_cfl_full(a, c->s) : fp32_cfl_full(a, c->s));
+        c->launches += 2;
+        c->cfl_valid = 1;
+    }
+    *grav_status = 1;
+    if (c->gravity) {
+        int st = f64 ? gravity_solve_dev(c, c->q64[c->cur][0], nullptr)
+                     : gravity_solve_dev(c, nullptr, c->q32[c->cur][0]);
+        if (st < -1) return st;
+        *grav_status = st;
+    }
+    HydroArgs a = hydro_args(c);
+    {
+        FamTimer t(c, FAM_BC);
+        CK(f64 ? fp64_dt(a, c->s) : fp32_dt(a, c->s));
+    }
+    {
+        FamTimer t(c, FAM_HYDRO);
+        CK(f64 ? fp64_interior(a, interior_chunks(c), c->s) : fp32_interior(a, interior_chunks(c), c->s));
+    }
+    {
+        FamTimer t(c, FAM_BC);
+        CK(f64 ? fp64_boundary_source(a, c->s) : fp32_boundary_source(a, c->s));
+        c->launches += 3;
+        for (int ax = 0; ax < 3; ax++)
+            if (c->cfg.bc[2 * ax] == 0 && c->cfg.bc[2 * ax + 1] == 0) {
+                CK(f64 ? fp64_periodic(a, ax, c->s) : fp32_periodic(a, ax, c->s));
+                c->launches++;
+            }
+        for (int ax = 0; ax < 3; ax++) {
+            CK(f64 ? fp64_bc(a, ax, c->s) : fp32_bc(a, ax, c->s));
+            c->launches++;
+        }
+        CK(f64 ? fp64_cfl_boundary(a, c->s) : fp32_cfl_boundary(a, c->s));
+        c->launches++;
+    }
+    c->hydro_launches++;
+    c->cur ^= 1;
+    c->parity ^= 1;
+    c->diag.steps++;
+    return HC_OK;
+}
+
+static int ensure_hdt(hc_ctx *c, int n)
+{
+    if (c->hdt && c->hdt_cap >= n) return HC_OK;
+    if (c->hdt) cudaFreeHost(c->hdt);
+    c->hdt = nullptr;
+    int cap = std::max(n, 64);
+    if (cudaMallocHost((void **)&c->hdt, cap * sizeof(double)) != cudaSuccess)
+        return set_err(HC_ERR_NOMEM, "pinned dt buffer");
+    c->hdt_cap = cap;
+    return HC_OK;
+}
+
+extern "C" int hc_step(hc_ctx *c, int nsteps, double *dt_out)
+{
+    if (!c || nsteps < 0) return set_err(HC_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = ensure_hdt(c, nsteps);
+    if (rc) return rc;
+    int worst = 0;
+    for (int q = 0; q < nsteps; q++) {
+        int gs = 1;
+        rc = step_once(c, &gs);
+        if (rc) return rc;
+        if (gs == -1) worst = -1;
+        CK(cudaMemcpyAsync(c->hdt + q, &c->sc->dt, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    }
+    rc = sync_ctx(c);
+    if (rc) return rc;
+    if (nsteps > 0) c->diag.dt = c->hdt[nsteps - 1];
+    if (dt_out)
+        for (int q = 0; q < nsteps; q++) dt_out[q] = c->hdt[q];
+    return worst ? HC_NOT_CONVERGED : HC_OK;
+}
+
+extern "C" int hc_step_host(hc_ctx *c, double *U, double *dt_out)
+{
+    if (!c || !U) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    rc = ensure_hdt(c, 1);
+    if (rc) return rc;
+    const size_t n = (size_t)c->g.n;
+    CK(cudaMemcpyAsync(c->stage, U, 5 * n * sizeof(double), cudaMemcpyHostToDevice, c->s));
+    if (c->cfg.precision == HC_FP64) CK(fp64_aos_to_soa(c->stage, c->q64[c->cur], c->g.n, c->s));
+    else CK(fp32_from_aos64(c->stage, c->q32[c->cur], c->g.n, c->s));
+    c->cfl_valid = 0;
+    int gs = 1;
+    rc = step_once(c, &gs);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->hdt, &c->sc->dt, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    if (c->cfg.precision == HC_FP64) CK(fp64_soa_to_aos(c->q64[c->cur], c->stage, c->g.n, c->s));
+    else CK(fp32_to_aos64(c->q32[c->cur], c->stage, c->g.n, c->s));
+    CK(cudaMemcpyAsync(U, c->stage, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    rc = sync_ctx(c);
+    if (rc) return rc;
+    c->diag.dt = c->hdt[0];
+    if (dt_out) *dt_out = c->hdt[0];
+    return gs == -1 ? HC_NOT_CONVERGED : HC_OK;
+}
+
+extern "C" int hc_get_diag(hc_ctx *c, hc_diag *d)
+{
+    if (!c || !d) return set_err(HC_ERR_ARG, "null argument");
+    *d = c->diag;
+    return HC_OK;
+}
+
+extern "C" int hc_get_timing(hc_ctx *c, hc_timing *t, int reset)
+{
+    if (!c || !t) return set_err(HC_ERR_ARG, "null argument");
+    int rc = sync_ctx(c);
+    if (rc) return rc;
+    t->hydro_ms = c->fam_ms[FAM_HYDRO];
+    t->bc_ms = c->fam_ms[FAM_BC];
+    t->sor_ms = c->fam_ms[FAM_SOR];
+    t->residual_ms = c->fam_ms[FAM_RES];
+    t->moments_ms = c->fam_ms[FAM_MOM];
+    t->unet_ms = c->fam_ms[FAM_UNET];
+    t->hydro_launches = c->hydro_launches;
+    t->sor_launches = c->sor_launches;
+    t->launches = c->launches;
+    if (reset) {
+        for (int f = 0; f < FAM_N; f++) c->fam_ms[f] = 0.0;
+        c->hydro_launches = c->sor_launches = c->launches = 0;
+    }
+    return HC_OK;
+}
+
+extern "C" int hc_sync(hc_ctx *c)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    CK(cudaSetDevice(c->dev));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_timer_start(hc_ctx *c)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    CK(cudaSetDevice(c->dev));
+    if (!c->t0) CK(cudaEventCreate(&c->t0));
+    if (!c->t1) CK(cudaEventCreate(&c->t1));
+    CK(cudaEventRecord(c->t0, c->s));
+    c->timer_on = 1;
+    return HC_OK;
+}
+
+extern "C" int hc_timer_stop(hc_ctx *c, double *ms)
+{
+    if (!c || !ms) return set_err(HC_ERR_ARG, "null argument");
+    if (!c->timer_on) return set_err(HC_ERR_STATE, "timer not started");
+    CK(cudaSetDevice(c->dev));
+    CK(cudaEventRecord(c->t1, c->s));
+    CK(cudaEventSynchronize(c->t1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, c->t0, c->t1));
+    *ms = f;
+    c->timer_on = 0;
+    return sync_ctx(c);
+}
+
+extern "C" int hc_host_register(void *ptr, size_t bytes)
+{
+    if (!ptr || !bytes) return set_err(HC_ERR_ARG, "null buffer");
+    CK(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    return HC_OK;
+}
+
+extern "C" int hc_host_unregister(void *ptr)
+{
+    if (!ptr) return set_err(HC_ERR_ARG, "null buffer");
+    CK(cudaHostUnregister(ptr));
+    return HC_OK;
+}

@@ -1,0 +1,169 @@
+// hc_internal.cuh -- device context and kernel entry points shared by the
+// translation units of the B200 hydro + gravity library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hydrocode_b200.h"
+
+namespace hc {
+
+// Grid geometry as the kernels see it.
+struct Geom {
+    int nx, ny, nz;
+    long long n;               // nx*ny*nz
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double dx, dy, dz;         // (max-min)/n, hydro_solver_3d.c:55-57
+};
+
+// Bitwise-ordered atomic max of a non-negative double (the bit pattern of a
+// non-negative IEEE double grows with its value).
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *slot, double v)
+{
+    atomicMax(slot, (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_max_nonneg(unsigned int *slot, float v)
+{
+    atomicMax(slot, (unsigned int)__float_as_uint(v));
+}
+
+// Device scalars of one context (one cudaMalloc'd struct).
+struct DevScalars {
+    unsigned long long smax[2];   // CFL max signal speed (bits), ping-pong per step
+    double dt;                    // current step dt
+    int done;                     // SOR converged / stopped flag
+    int last_iter;                // iterations of the finished solve
+    int overshoot;                // temporal blocking passed tol inside a pass
+    int err;                      // sticky device error code
+    unsigned long long resid_bits; // scratch
+    double moments[4 + 9];        // M, COM, Q (reference mode)
+    double resnorm;               // post-hoc residual
+};
+
+// Boundary-cell enumeration: index t in [0, nb) -> (i,j,k) on the faces.
+// zb: whether the z faces are boundary (false in the nz == 1 gravity mode).
+__host__ __device__ __forceinline__ long long boundary_count(int nx, int ny, int nz, bool zb)
+{
+    if (zb) return 2LL * ny * nz + 2LL * (nx - 2) * nz + 2LL * (nx - 2) * (ny - 2);
+    return (2LL * ny + 2LL * (nx - 2)) * nz;
+}
+__device__ __forceinline__ void boundary_cell(long long t, int nx, int ny, int nz, bool zb,
+                                              int &i, int &j, int &k)
+{
+    long long a = 2LL * ny * nz;
+    if (t < a) {
+        i = (t < (long long)ny * nz) ? 0 : nx - 1;
+        long long r = t % ((long long)ny * nz);
+        j = (int)(r / nz); k = (int)(r % nz);
+        return;
+    }
+    t -= a;
+    long long b = 2LL * (nx - 2) * nz;
+    if (t < b) {
+        j = (t < (long long)(nx - 2) * nz) ? 0 : ny - 1;
+        long long r = t % ((long long)(nx - 2) * nz);
+        i = 1 + (int)(r / nz); k = (int)(r % nz);
+        return;
+    }
+    t -= b;
+    // z faces (only when zb)
+    k = (t < (long long)(nx - 2) * (ny - 2)) ? 0 : nz - 1;
+    long long r = t % ((long long)(nx - 2) * (ny - 2));
+    i = 1 + (int)(r / (ny - 2)); j = 1 + (int)(r % (ny - 2));
+}
+
+}  // namespace hc
+
+// ---------------------------------------------------------------------------
+// Launchers implemented in the kernel translation units (host functions).
+// All take the context's stream and return cudaError_t of the launch.
+// ---------------------------------------------------------------------------
+namespace hc {
+
+struct HydroArgs {
+    Geom g;
+    double gamma, cfl;
+    int bc[6];
+    int gravity;
+    const void *qin[5];     // double* or float* per precision
+    void *qout[5];
+    const double *phig;     // potential used for g (last converged)
+    DevScalars *sc;
+    int step_parity;        // smax slot read = parity, written = parity^1
+};
+
+// FP64 (bit-exact) hydro path -- hydro_fp64.cu
+cudaError_t fp64_cfl_full(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp64_dt(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp64_interior(const HydroArgs &a, int chunks, cudaStream_t s);
+cudaError_t fp64_boundary_source(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp64_periodic(const HydroArgs &a, int axis, cudaStream_t s);
+cudaError_t fp64_bc(const HydroArgs &a, int axis, cudaStream_t s);
+cudaError_t fp64_cfl_boundary(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp64_aos_to_soa(const double *aos, double *const q[5], long long n, cudaStream_t s);
+cudaError_t fp64_soa_to_aos(const double *const q[5], double *aos, long long n, cudaStream_t s);
+
+// FP32 hydro path -- hydro_fp32.cu
+cudaError_t fp32_cfl_full(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp32_dt(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp32_interior(const HydroArgs &a, int chunks, cudaStream_t s);
+cudaError_t fp32_boundary_source(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp32_periodic(const HydroArgs &a, int axis, cudaStream_t s);
+cudaError_t fp32_bc(const HydroArgs &a, int axis, cudaStream_t s);
+cudaError_t fp32_cfl_boundary(const HydroArgs &a, cudaStream_t s);
+cudaError_t fp32_from_fp64(const double *const q64[5], float *const q32[5], long long n, cudaStream_t s);
+cudaError_t fp32_to_fp64(const float *const q32[5], double *const q64[5], long long n, cudaStream_t s);
+cudaError_t f32_to_f64(const float *a, double *b, long long n, cudaStream_t s);
+cudaError_t fp32_from_aos64(const double *aos, float *const q[5], long long n, cudaStream_t s);
+cudaError_t fp32_to_aos64(const float *const q[5], double *aos, long long n, cudaStream_t s);
+
+struct GravArgs {
+    Geom g;
+    double G, omega, tol;
+    int max_iter;
+    int grav_bc;
+    int lmax;
+    int moment_order;
+    double *phi;
+    const double *rho;        // FP64 density (parity path)
+    const float *rho32;       // FP32 density (mixed path) -- used when rho == NULL
+    double *res;              // per-iteration residual slots (bits), max_iter+1
+    DevScalars *sc;
+    double *scratch;          // moment partial sums
+    long long scratch_len;
+    double *mom;              // multipole results: 4 + ncoef
+    double *gx, *gy, *gz;
+};
+
+// FP64 gravity (bit-exact) -- gravity_fp64.cu
+cudaError_t grav_moments_sequential(const GravArgs &a, cudaStream_t s);
+cudaError_t grav_moments_tree(const GravArgs &a, cudaStream_t s);
+cudaError_t grav_boundary_ref(const GravArgs &a, cudaStream_t s);
+cudaError_t grav_boundary_periodic(const GravArgs &a, cudaStream_t s);
+cudaError_t grav_sor_color(const GravArgs &a, int color, int iter, cudaStream_t s);
+cudaError_t grav_sor_wavefront(const GravArgs &a, int iter0, int depth, cudaStream_t s);
+cudaError_t grav_check(const GravArgs &a, int iter, cudaStream_t s);
+cudaError_t grav_accel(const GravArgs &a, cudaStream_t s);
+cudaError_t grav_residual_norm(const GravArgs &a, const double *phi, cudaStream_t s);
+cudaError_t grav_reset_slots(const GravArgs &a, int from, int count, cudaStream_t s);
+
+// Multipole to lmax and mixed precision -- gravity_mixed.cu
+cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s);
+cudaError_t grav_boundary_lmax(const GravArgs &a, cudaStream_t s);
+int lmax_ncoef(int lmax);
+
+}  // namespace hc
+
+namespace hc {
+cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, cudaStream_t s);
+cudaError_t mixed_update(const GravArgs &a, const float *e32, cudaStream_t s);
+cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int color, int iter,
+                        double thresh, cudaStream_t s);
+cudaError_t mixed_check(const GravArgs &a, int iter, double thresh, cudaStream_t s);
+}  // namespace hc
+
+namespace hc {
+cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, int iter0, cudaStream_t s);
+cudaError_t mixed_sor32_pass(const GravArgs &a, const float *in, float *out, const float *r32, int iter0,
+                             int depth, double thresh, cudaStream_t s);
+}  // namespace hc

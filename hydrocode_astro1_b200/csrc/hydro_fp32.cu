@@ -1,0 +1,149 @@
+// hydro_fp32.cu -- FP32 instantiation of the hydro step kernels (FP32 state
+// and HLLC arithmetic; the potential and g stay FP64).
+#include "hydro_kernels.cuh"
+
+namespace hc {
+
+namespace {
+constexpr int TK = 32, TJ = 8;
+__global__ void set_smax32(DevScalars *sc, int slot)
+{
+    sc->smax[slot] = (unsigned long long)__float_as_uint(1.0e-10f);
+}
+__global__ void cvt_to32(const double *a0, const double *a1, const double *a2, const double *a3,
+                         const double *a4, float *b0, float *b1, float *b2, float *b3, float *b4,
+                         long long n)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        b0[c] = (float)a0[c]; b1[c] = (float)a1[c]; b2[c] = (float)a2[c];
+        b3[c] = (float)a3[c]; b4[c] = (float)a4[c];
+    }
+}
+__global__ void cvt_to64(const float *a, double *b, long long n)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+        b[c] = (double)a[c];
+}
+inline int grid_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+}  // namespace
+
+cudaError_t fp32_cfl_full(const HydroArgs &a, cudaStream_t s)
+{
+    set_smax32<<<1, 1, 0, s>>>(a.sc, a.step_parity);
+    cfl_full_kernel<float><<<148 * 8, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_dt(const HydroArgs &a, cudaStream_t s)
+{
+    dt_kernel<float><<<1, 1, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_interior(const HydroArgs &a, int chunks, cudaStream_t s)
+{
+    constexpr size_t sm = interior_smem<float, TK, TJ>();
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(interior_kernel<float, TK, TJ>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    int nint = a.g.nx - 2;
+    int ilen = (nint + chunks - 1) / chunks;
+    chunks = (nint + ilen - 1) / ilen;
+    dim3 grid((a.g.nz + TK - 1) / TK, (a.g.ny + TJ - 1) / TJ, chunks);
+    interior_kernel<float, TK, TJ><<<grid, dim3(TK, TJ), sm, s>>>(a, ilen);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_boundary_source(const HydroArgs &a, cudaStream_t s)
+{
+    long long nb = boundary_count(a.g.nx, a.g.ny, a.g.nz, true);
+    boundary_source_kernel<float><<<grid_for(nb, 256), 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+static long long face_count(const HydroArgs &a, int axis)
+{
+    const int n[3] = { a.g.nx, a.g.ny, a.g.nz };
+    return (long long)((axis == 0) ? n[1] : n[0]) * ((axis == 2) ? n[1] : n[2]);
+}
+
+cudaError_t fp32_periodic(const HydroArgs &a, int axis, cudaStream_t s)
+{
+    periodic_kernel<float><<<grid_for(face_count(a, axis), 256), 256, 0, s>>>(a, axis);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_bc(const HydroArgs &a, int axis, cudaStream_t s)
+{
+    bc_kernel<float><<<grid_for(face_count(a, axis), 256), 256, 0, s>>>(a, axis);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_cfl_boundary(const HydroArgs &a, cudaStream_t s)
+{
+    long long nb = boundary_count(a.g.nx, a.g.ny, a.g.nz, true);
+    int blocks = (int)std::min<long long>(grid_for(nb, 256), 148 * 4);
+    cfl_boundary_kernel<float><<<blocks, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_from_fp64(const double *const q64[5], float *const q32[5], long long n, cudaStream_t s)
+{
+    cvt_to32<<<148 * 8, 256, 0, s>>>(q64[0], q64[1], q64[2], q64[3], q64[4], q32[0], q32[1], q32[2],
+                                     q32[3], q32[4], n);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_to_fp64(const float *const q32[5], double *const q64[5], long long n, cudaStream_t s)
+{
+    for (int v = 0; v < 5; v++) cvt_to64<<<148 * 8, 256, 0, s>>>(q32[v], q64[v], n);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void aos64_to_soa32(const double *aos, float *q0, float *q1, float *q2, float *q3, float *q4,
+                               long long n)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        const double *p = aos + 5 * c;
+        q0[c] = (float)p[0]; q1[c] = (float)p[1]; q2[c] = (float)p[2];
+        q3[c] = (float)p[3]; q4[c] = (float)p[4];
+    }
+}
+__global__ void soa32_to_aos64(const float *q0, const float *q1, const float *q2, const float *q3,
+                               const float *q4, double *aos, long long n)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        double *p = aos + 5 * c;
+        p[0] = q0[c]; p[1] = q1[c]; p[2] = q2[c]; p[3] = q3[c]; p[4] = q4[c];
+    }
+}
+}  // namespace
+
+cudaError_t fp32_from_aos64(const double *aos, float *const q[5], long long n, cudaStream_t s)
+{
+    aos64_to_soa32<<<148 * 8, 256, 0, s>>>(aos, q[0], q[1], q[2], q[3], q[4], n);
+    return cudaGetLastError();
+}
+
+cudaError_t fp32_to_aos64(const float *const q[5], double *aos, long long n, cudaStream_t s)
+{
+    soa32_to_aos64<<<148 * 8, 256, 0, s>>>(q[0], q[1], q[2], q[3], q[4], aos, n);
+    return cudaGetLastError();
+}
+
+cudaError_t f32_to_f64(const float *a, double *b, long long n, cudaStream_t s)
+{
+    cvt_to64<<<148 * 8, 256, 0, s>>>(a, b, n);
+    return cudaGetLastError();
+}
+
+}  // namespace hc

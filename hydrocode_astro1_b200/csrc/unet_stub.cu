@@ -1,0 +1,5 @@
+// unet_stub.cu -- placeholder for the learned warm start.
+#include "hc_internal.cuh"
+void hc_unet_free(void *) {}
+extern "C" int hc_unet_param_count(void) { return 0; }
+extern "C" int hc_unet_load(hc_ctx *, const uint16_t *, int) { return HC_ERR_STATE; }

@@ -1,0 +1,192 @@
+/*
+ * hydrocode_b200.h -- C ABI of the B200 (sm_100a) hydro + self-gravity step.
+ *
+ * Plain C types only: pointers, sizes, ints, doubles.  One context object
+ * owns all device memory of one solver; the host keeps the reference's
+ * array-of-structures State3D layout (5 doubles per cell, IDX3D row-major
+ * with k fastest, hydro_solver_3d.h:12-21) at this boundary, while the device
+ * stores structure-of-arrays fields.
+ *
+ * Every function returns HC_OK (0) or a negative HC_ERR_* code; the message
+ * of the last error of the calling thread is available from hc_last_error().
+ * A context is used by one host thread at a time (the reference solver is
+ * single-threaded and non-reentrant, gravity_solver_3d.c:552).
+ *
+ * Reference interfaces these entry points replace (file:line in the
+ * reference project):
+ *   hc_create / hc_destroy            solver3d_create + gravity_solver_create,
+ *                                     solver3d_destroy (hydro_solver_3d.c:33-128,
+ *                                     gravity_solver_3d.c:49-131)
+ *   hc_step                           godunov_step_3d (hydro_solver_3d.c:637-811),
+ *                                     the body of the run loops (:2257-2275)
+ *   hc_step_host                      the same step on a host State3D array
+ *   hc_gravity_solve                  gravity_solve / gravity_solve_potential
+ *                                     (gravity_solver_3d.c:905-911, :510-747)
+ *   hc_gravity_acceleration           gravity_compute_acceleration (:753-899)
+ *   hc_set_gravity_params             gravity_set_solver_params (:137-144)
+ *   hc_set_gravity_bc                 gravity_set_boundary_type (:146-148)
+ *   hc_get_diag                       gravity_get_diagnostics (:150-155)
+ *   hc_set_state / hc_get_state       the U array the reference steps in place
+ *   hc_get_phi / hc_get_accel         GravitySolver3D.phi / gx gy gz
+ */
+#ifndef HYDROCODE_B200_H
+#define HYDROCODE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hc_ctx hc_ctx;
+
+enum {
+    HC_OK = 0,
+    HC_NOT_CONVERGED = -1,   /* SOR hit max_iter (gravity_solver_3d.c:746) */
+    HC_ERR_ARG = -2,
+    HC_ERR_CUDA = -3,
+    HC_ERR_NOMEM = -4,
+    HC_ERR_STATE = -5,
+    HC_ERR_TIMEOUT = -6,     /* a bounded device wait gave up */
+    HC_ERR_NUMERIC = -7      /* non-finite value met */
+};
+
+/* Arithmetic of the step. */
+enum {
+    HC_FP64 = 0,    /* FP64 throughout, reference operation order, no FMA:
+                       bit-identical to the reference C build */
+    HC_FP32 = 1     /* FP32 hydro state and HLLC, FP64 potential with FP64
+                       residual and FP32 SOR correction sweeps */
+};
+
+/* Order of the FP64 multipole moment sums. */
+enum {
+    HC_MOMENTS_SEQUENTIAL = 0,  /* the reference's (i,j,k) order: bit-exact */
+    HC_MOMENTS_TREE = 1         /* deterministic parallel tree */
+};
+
+/* Warm start of each Poisson solve. */
+enum {
+    HC_WARM_PREVIOUS = 0,   /* previous step's potential (the reference) */
+    HC_WARM_UNET = 1        /* learned 3D U-Net prediction, checked against
+                               the previous potential */
+};
+
+typedef struct hc_config {
+    int nx, ny, nz;
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    double gamma;            /* adiabatic index */
+    double cfl;
+    double G;                /* self-gravity on iff G > 0 (hydro_solver_3d.c:63) */
+    int bc[6];               /* BCType (0 periodic, 1 reflective, 2 outflow):
+                                xmin, xmax, ymin, ymax, zmin, zmax */
+    int precision;           /* HC_FP64 / HC_FP32 */
+    int moment_order;        /* HC_MOMENTS_* */
+    int grav_bc;             /* GravBCType: 0 periodic, 1 isolated, 2 dirichlet */
+    int lmax;                /* 0: reference monopole + Cartesian quadrupole;
+                                1..12: real solid harmonics to degree lmax */
+    double omega;            /* SOR relaxation (default 1.5) */
+    double tol;              /* SOR tolerance on max |phi_GS - phi_old| */
+    int max_iter;
+    int sor_depth;           /* SOR iterations per HBM pass (temporal blocking);
+                                0 selects the default */
+    int warm_start;          /* HC_WARM_* */
+    int device;              /* CUDA device ordinal */
+    int gravity_only;        /* 1: Poisson solver only (no hydro state); allows
+                                nz == 1, the reference's 2D mode */
+} hc_config;
+
+typedef struct hc_diag {
+    int last_iterations;     /* iterations of the last solve */
+    double last_residual;    /* its final update norm */
+    int last_status;         /* 0 converged, -1 not converged */
+    int warm_start_used;     /* 1 if the learned start was taken */
+    int outer_cycles;        /* mixed precision: FP64 residual evaluations */
+    double dt;               /* dt of the last step */
+    long long steps;         /* steps taken by this context */
+    long long total_iterations;
+    int overshoot;           /* temporal blocking crossed tol inside a pass */
+} hc_diag;
+
+/* Per-kernel-family device time (CUDA events on the context's stream),
+ * accumulated since the last reset, in milliseconds. */
+typedef struct hc_timing {
+    double hydro_ms;         /* fused flux/update/source kernel */
+    double bc_ms;            /* boundary source, periodic copies, BCs, CFL */
+    double sor_ms;           /* SOR sweeps (and FP32 correction sweeps) */
+    double residual_ms;      /* FP64 residual + correction update */
+    double moments_ms;       /* multipole moments + boundary evaluation */
+    double unet_ms;          /* learned warm start */
+    long long hydro_launches;
+    long long sor_launches;
+    long long launches;      /* every kernel launched by this context */
+} hc_timing;
+
+void hc_config_default(hc_config *cfg);
+
+hc_ctx *hc_create(const hc_config *cfg);
+void hc_destroy(hc_ctx *ctx);
+
+size_t hc_ncells(const hc_ctx *ctx);
+
+/* Conserved state, host array of ncells State3D (5 doubles per cell). */
+int hc_set_state(hc_ctx *ctx, const double *U_aos);
+int hc_get_state(hc_ctx *ctx, double *U_aos);
+/* Conserved state as 5 consecutive fields of ncells doubles. */
+int hc_set_state_soa(hc_ctx *ctx, const double *q);
+int hc_get_state_soa(hc_ctx *ctx, double *q);
+
+/* nsteps godunov steps on the device-resident state; dt_out (nullable)
+ * receives each step's dt.  Returns HC_OK, or HC_NOT_CONVERGED if any SOR
+ * solve failed (the step still completes, as in the reference). */
+int hc_step(hc_ctx *ctx, int nsteps, double *dt_out);
+
+/* One step on a host State3D array: upload, step, download. */
+int hc_step_host(hc_ctx *ctx, double *U_aos, double *dt_out);
+
+/* Poisson solve for a host density (rho != NULL) or the current state's
+ * density (rho == NULL).  with_accel: also form g on success, as
+ * gravity_solve does. */
+int hc_gravity_solve(hc_ctx *ctx, const double *rho, int with_accel);
+int hc_gravity_acceleration(hc_ctx *ctx);
+int hc_set_gravity_params(hc_ctx *ctx, double omega, int max_iter, double tol);
+int hc_set_gravity_bc(hc_ctx *ctx, int grav_bc);
+
+int hc_get_phi(hc_ctx *ctx, double *phi);
+int hc_set_phi(hc_ctx *ctx, const double *phi);
+int hc_get_accel(hc_ctx *ctx, double *gx, double *gy, double *gz);
+
+/* Multipole data of the last solve: mom[0]=M, mom[1..3]=centre of mass,
+ * then 9 Cartesian Q (lmax == 0) or (lmax+1)^2 solid-harmonic moments. */
+int hc_get_moments(hc_ctx *ctx, double *mom, int cap);
+
+/* FP64 max |(lap_nbrs(phi) - 4 pi G rho)/factor - phi| over the interior. */
+int hc_residual_norm(hc_ctx *ctx, double *out);
+
+int hc_get_diag(hc_ctx *ctx, hc_diag *d);
+int hc_get_timing(hc_ctx *ctx, hc_timing *t, int reset);
+int hc_sync(hc_ctx *ctx);
+
+/* Device time between two points of the context's stream (CUDA events on
+ * that stream): hc_timer_start records the start, hc_timer_stop the end,
+ * waits for it and returns the elapsed milliseconds. */
+int hc_timer_start(hc_ctx *ctx);
+int hc_timer_stop(hc_ctx *ctx, double *ms);
+
+/* Learned warm start: load weights (nparam BF16 values as uint16) or query
+ * the parameter count of the network built into this library. */
+int hc_unet_param_count(void);
+int hc_unet_load(hc_ctx *ctx, const uint16_t *w_bf16, int nparam);
+
+/* Page-lock (pin) a host buffer for faster transfers, and release it. */
+int hc_host_register(void *ptr, size_t bytes);
+int hc_host_unregister(void *ptr);
+
+const char *hc_last_error(void);
+int hc_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
