@@ -159,9 +159,12 @@ def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
     s = hc.HydroSolver3D(p["shape"], **solver_kwargs(p, variant, device))
     s.set_state(q0)
     warm_iters = []
-    for _ in range(warmup):
+    for w in range(warmup):
+        t = time.perf_counter()
         s.step(1)
         warm_iters.append(s.diagnostics()["last_iterations"])
+        log(f"[bench] {variant} warm-up step {w}: {time.perf_counter() - t:.3f} s, "
+            f"{warm_iters[-1]} SOR iterations")
     s.timing(reset=True)
     iters = []
     barrier(dist)
@@ -176,10 +179,15 @@ def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
         iters.append(s.diagnostics()["last_iterations"])
     ms = s.timer_stop()
     ck = clocks.stop() if clocks else None
+    log(f"[bench] {variant}: {steps} timed steps {ms:.1f} ms, SOR iterations {iters}")
     tm = s.timing()
     d = s.diagnostics()
     return dict(solver=s, ms=ms, iters=iters, warm_iters=warm_iters, timing=tm, diag=d,
                 dts=dts, clocks=ck, total_iters=d["total_iterations"] - d0)
+
+
+def log(msg):
+    print(msg, file=sys.stderr, flush=True)
 
 
 def peaks():
@@ -356,6 +364,7 @@ def main_ours(args):
         for _ in range(ne):
             s.step_host(U)
         te = time.perf_counter() - t
+        log(f"[bench] e2e: {ne} steps through hc_step_host in {te:.3f} s")
         te = reduce_max(dist, te)
         hc.unpin(U)
         line["e2e"] = {"value": ncell * ne * world / te / 1e6, "unit": UNIT,
@@ -367,7 +376,10 @@ def main_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.oracle import have_reference
         if have_reference():
+            t0 = time.perf_counter()
             th, tit = reference_sample(q0, p, sor_iters=5)
+            log(f"[bench] cpu baseline sample: hydro {th:.2f} s, SOR {tit * 1e3:.0f} ms/iteration "
+                f"({time.perf_counter() - t0:.1f} s total)")
             I = statistics.mean(r["iters"]) if fp64 else None
             if I is None:
                 I, _src = reference_iterations(args.n)

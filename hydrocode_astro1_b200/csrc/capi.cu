@@ -97,6 +97,7 @@ struct hc_ctx {
     // user timer
     cudaEvent_t t0, t1;
     int timer_on;
+    int debug;                   // HC_DEBUG=1: per-solve progress on stderr
 };
 
 static cudaEvent_t ev_get(hc_ctx *c)
@@ -328,6 +329,8 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
     c->cur = 0;
     c->parity = 0;
     c->cfl_valid = 0;
+    const char *dbg = getenv("HC_DEBUG");
+    c->debug = dbg && atoi(dbg) != 0;
     return c;
 }
 
@@ -362,6 +365,7 @@ static int upload_soa64(hc_ctx *c, const double *q)
 
 extern "C" int hc_set_state(hc_ctx *c, const double *U)
 {
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
     if (!c || !U) return set_err(HC_ERR_ARG, "null argument");
     CK(cudaSetDevice(c->dev));
     int rc = ensure_stage(c);
@@ -377,6 +381,7 @@ extern "C" int hc_set_state(hc_ctx *c, const double *U)
 
 extern "C" int hc_get_state(hc_ctx *c, double *U)
 {
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
     if (!c || !U) return set_err(HC_ERR_ARG, "null argument");
     CK(cudaSetDevice(c->dev));
     int rc = ensure_stage(c);
@@ -390,6 +395,7 @@ extern "C" int hc_get_state(hc_ctx *c, double *U)
 
 extern "C" int hc_set_state_soa(hc_ctx *c, const double *q)
 {
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
     if (!c || !q) return set_err(HC_ERR_ARG, "null argument");
     CK(cudaSetDevice(c->dev));
     int rc = upload_soa64(c, q);
@@ -399,6 +405,7 @@ extern "C" int hc_set_state_soa(hc_ctx *c, const double *q)
 
 extern "C" int hc_get_state_soa(hc_ctx *c, double *q)
 {
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
     if (!c || !q) return set_err(HC_ERR_ARG, "null argument");
     CK(cudaSetDevice(c->dev));
     const size_t n = (size_t)c->g.n;
@@ -597,11 +604,19 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         CK(cudaMemcpyAsync(&c->hsc->resnorm, &c->sc->resnorm, sizeof(double), cudaMemcpyDeviceToHost, c->s));
         rc = sync_ctx(c);
         if (rc) return rc;
+        const double prev_dmax = cycles ? dmax : 1e300;
         dmax = c->hsc->resnorm;
         cycles++;
+        if (c->debug) fprintf(stderr, "[hc] mixed cycle %d: max|delta| %.3e after %d sweeps\n", cycles, dmax, total);
         if (!std::isfinite(dmax)) return set_err(HC_ERR_NUMERIC, "non-finite Poisson residual");
         if (dmax < a.tol) { status = 0; break; }
         if (total >= a.max_iter) break;
+        // a correction cycle that does not halve the residual means the FP32
+        // sweeps cannot resolve it: report non-convergence instead of looping
+        if (dmax > 0.5 * prev_dmax) {
+            if (c->debug) fprintf(stderr, "[hc] mixed solve stalled at %.3e\n", dmax);
+            break;
+        }
         // one cycle reduces the residual 1e4-fold at most: FP32 resolves the
         // correction e to ~1e-7 |e|, and |e| can exceed max|delta| by the
         // grid's condition number on a cold start
@@ -656,7 +671,10 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
                 double v = c->hslots[q];
                 if (v > 0.0 && v < 0.995 * best) { best = v; best_it = end - nb + q; }
             }
-            if (end - best_it > 2048) break;
+            if (end - best_it > 2048) {
+                if (c->debug) fprintf(stderr, "[hc] inner sweeps stagnated at %.3e (thresh %.3e)\n", best, thresh);
+                break;
+            }
             it = end;
             batch = std::min(batch * 2, 256);
         }
@@ -709,6 +727,8 @@ extern "C" int hc_gravity_solve(hc_ctx *c, const double *rho, int with_accel)
         }
         CK(cudaMemcpyAsync(c->rho_ext, rho, n * sizeof(double), cudaMemcpyHostToDevice, c->s));
         st = gravity_solve_dev(c, c->rho_ext, nullptr);
+    } else if (c->cfg.gravity_only) {
+        return set_err(HC_ERR_ARG, "gravity-only context: pass a density");
     } else if (c->cfg.precision == HC_FP64) {
         st = gravity_solve_dev(c, c->q64[c->cur][0], nullptr);
     } else {
@@ -819,8 +839,10 @@ extern "C" int hc_residual_norm(hc_ctx *c, double *out)
     if (!c || !out) return set_err(HC_ERR_ARG, "null argument");
     if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled");
     CK(cudaSetDevice(c->dev));
-    GravArgs a = c->cfg.precision == HC_FP64 ? grav_args(c, c->q64[c->cur][0], nullptr)
-                                             : grav_args(c, nullptr, c->q32[c->cur][0]);
+    if (c->cfg.gravity_only && !c->rho_ext) return set_err(HC_ERR_STATE, "no density solved for yet");
+    GravArgs a = c->cfg.gravity_only ? grav_args(c, c->rho_ext, nullptr)
+                 : c->cfg.precision == HC_FP64 ? grav_args(c, c->q64[c->cur][0], nullptr)
+                                               : grav_args(c, nullptr, c->q32[c->cur][0]);
     CK(cudaMemsetAsync(&c->sc->resnorm, 0, sizeof(double), c->s));
     CK(grav_residual_norm(a, c->phi, c->s));
     CK(cudaMemcpyAsync(&c->hsc->resnorm, &c->sc->resnorm, sizeof(double), cudaMemcpyDeviceToHost, c->s));
@@ -954,6 +976,7 @@ extern "C" int hc_step(hc_ctx *c, int nsteps, double *dt_out)
 
 extern "C" int hc_step_host(hc_ctx *c, double *U, double *dt_out)
 {
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
     if (!c || !U) return set_err(HC_ERR_ARG, "null argument");
     CK(cudaSetDevice(c->dev));
     int rc = ensure_stage(c);

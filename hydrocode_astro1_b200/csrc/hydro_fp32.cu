@@ -1,6 +1,12 @@
 // hydro_fp32.cu -- FP32 instantiation of the hydro step kernels (FP32 state
 // and HLLC arithmetic; the potential and g stay FP64).
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdlib>
+
 #include "hydro_kernels.cuh"
+#include "hydro_fp32_tma.cuh"
 
 namespace hc {
 
@@ -42,8 +48,61 @@ cudaError_t fp32_dt(const HydroArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// TMA tensor map over the five FP32 fields of a state buffer:
+// dims (k, j, i, field), box (40, 10, 1, 5) -- one plane tile with halo.
+static cudaError_t encode_state_map(const HydroArgs &a, CUtensorMap *tm)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t n = (cuuint64_t)a.g.n;
+    cuuint64_t dims[4] = { (cuuint64_t)a.g.nz, (cuuint64_t)a.g.ny, (cuuint64_t)a.g.nx, 5 };
+    cuuint64_t strides[3] = { (cuuint64_t)a.g.nz * 4, (cuuint64_t)a.g.ny * a.g.nz * 4, n * 4 };
+    cuuint32_t box[4] = { (cuuint32_t)tma32::RK, (cuuint32_t)tma32::RJ, 1, 5 };
+    cuuint32_t es[4] = { 1, 1, 1, 1 };
+    CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(a.qin[0]), dims, strides, box,
+                     es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+static bool tma_usable(const HydroArgs &a)
+{
+    static int off = -1;
+    if (off < 0) {
+        const char *e = getenv("HC_NO_TMA");
+        off = (e && atoi(e) != 0) ? 1 : 0;
+    }
+    // row and field strides must be multiples of 16 bytes; fields contiguous
+    return !off && (a.g.nz % 4) == 0 &&
+           (const float *)a.qin[1] == (const float *)a.qin[0] + a.g.n &&
+           (const float *)a.qin[4] == (const float *)a.qin[0] + 4 * a.g.n &&
+           ((uintptr_t)a.qin[0] % 16) == 0;
+}
+
 cudaError_t fp32_interior(const HydroArgs &a, int chunks, cudaStream_t s)
 {
+    if (tma_usable(a)) {
+        CUtensorMap tm;
+        cudaError_t e = encode_state_map(a, &tm);
+        if (e == cudaSuccess) {
+            // 3 CTAs per SM, about 4 waves
+            long long tiles = (long long)((a.g.nz + tma32::TK - 1) / tma32::TK) * ((a.g.ny + tma32::TJ - 1) / tma32::TJ);
+            long long want = 148LL * 3 * 4;
+            int nint = a.g.nx - 2;
+            int ch = (int)std::max(1LL, std::min((want + tiles - 1) / tiles, (long long)std::max(1, nint / 8)));
+            int ilen = (nint + ch - 1) / ch;
+            ch = (nint + ilen - 1) / ilen;
+            dim3 grid((a.g.nz + tma32::TK - 1) / tma32::TK, (a.g.ny + tma32::TJ - 1) / tma32::TJ, ch);
+            tma32::interior_tma_kernel<<<grid, dim3(tma32::TK, tma32::TJ), 0, s>>>(tm, a, ilen);
+            return cudaGetLastError();
+        }
+    }
     constexpr size_t sm = interior_smem<float, TK, TJ>();
     static bool attr = false;
     if (!attr) {
