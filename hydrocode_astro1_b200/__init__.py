@@ -96,6 +96,9 @@ CAPI = {
     "hc_timer_stop": (C.c_int, [C.c_void_p, _dp]),
     "hc_unet_param_count": (C.c_int, []),
     "hc_unet_load": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint16), C.c_int]),
+    "hc_sor_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                        C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        C.c_double, C.c_void_p, C.POINTER(C.c_int), _dp]),
     "hc_host_register": (C.c_int, [C.c_void_p, C.c_size_t]),
     "hc_host_unregister": (C.c_int, [C.c_void_p]),
     "hc_last_error": (C.c_char_p, []),

@@ -1075,3 +1075,9 @@ extern "C" int hc_host_unregister(void *ptr)
     CK(cudaHostUnregister(ptr));
     return HC_OK;
 }
+
+// Error reporting for entry points defined in other translation units.
+int hc_internal_set_error(int code, const char *msg)
+{
+    return set_err(code, "%s", msg);
+}

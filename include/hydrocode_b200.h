@@ -179,6 +179,36 @@ int hc_timer_stop(hc_ctx *ctx, double *ms);
 int hc_unet_param_count(void);
 int hc_unet_load(hc_ctx *ctx, const uint16_t *w_bf16, int nparam);
 
+/* Red-black SOR to tolerance on caller-owned DEVICE arrays, allocating
+ * nothing.  No counterpart in the reference: it exists for callers that own
+ * all device memory themselves (a fixed arena reserved at start-up, a pool
+ * shared with other solvers, a budget that must not grow or fail with
+ * out-of-memory mid-run) and for callers whose other streams must not see
+ * the device-wide synchronisation that cudaMalloc/cudaFree can cause.
+ *
+ * phi (nx*ny*nz doubles, in/out) is iterated in place on the interior; its
+ * boundary cells are held as given.  rho is read only.  Arithmetic and stop
+ * rule are those of hc_gravity_solve (max |phi_GS - phi_old| < tol), so the
+ * iterates match it bit for bit.  `stream` is a cudaStream_t (NULL: the
+ * legacy default stream); the call returns after the solve has finished on
+ * it.  Returns HC_OK, HC_NOT_CONVERGED, HC_ERR_ARG (max_iter outside
+ * 1..HC_NOALLOC_MAX_ITER, a dimension below 3, null or non-positive inputs)
+ * or HC_ERR_CUDA.
+ *
+ * Scratch: one residual slot per iteration plus two flags live in a fixed
+ * file-scope device array of (HC_NOALLOC_MAX_ITER + 8) * 8 bytes (about
+ * 512 KB) that every GPU loading this library holds until the process exits;
+ * max_iter above HC_NOALLOC_MAX_ITER is rejected.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current: make that first call before any stream capture.  Every call shares
+ * the array and clears what it needs at its start, so calls that overlap on
+ * the GPU (concurrent streams, threads) race: serialise them. */
+#define HC_NOALLOC_MAX_ITER 65536
+int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int ny, int nz,
+                         double dx, double dy, double dz, double G, double omega,
+                         int max_iter, double tol, void *stream,
+                         int *iterations, double *residual);
+
 /* Page-lock (pin) a host buffer for faster transfers, and release it. */
 int hc_host_register(void *ptr, size_t bytes);
 int hc_host_unregister(void *ptr);
