@@ -514,10 +514,23 @@ cudaError_t grav_reset_slots(const GravArgs &a, int from, int count, cudaStream_
 // One full red-black iteration per pass over HBM (wavefront, out of place).
 // ---------------------------------------------------------------------------
 #include "sor_wavefront.cuh"
+#include "sor_wavefront_tma.cuh"
+#include "tmap.cuh"
 
 namespace hc {
 namespace {
 constexpr int WF64_T = 1, WF64_TJ = 16, WF64_TK = 64, WF64_NT = 256;
+}
+
+// HC_NO_TMA=1 selects the plain-load kernels (A/B comparisons).
+bool wf_tma_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("HC_NO_TMA");
+        on = (e && atoi(e) != 0) ? 0 : 1;
+    }
+    return on == 1;
 }
 
 cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, int iter0, cudaStream_t s)
@@ -548,6 +561,21 @@ cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, in
     int chunk = (nint + chunks - 1) / chunks;
     chunks = (nint + chunk - 1) / chunk;
     dim3 grid(tk, tj, chunks);
+    // operands staged by TMA where the layout allows it (16-byte row stride)
+    using SH = wtma::Shape<double, WF64_T, WF64_TJ, WF64_TK>;
+    CUtensorMap tin, tsrc;
+    if (wf_tma_enabled() && tmap3(in, 8, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tin) &&
+        tmap3(a.rho, 8, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tsrc)) {
+        auto kt = wtma::sor_wavefront_tma_kernel<double, double, WF64_T, WF64_TJ, WF64_TK, WF64_NT>;
+        static int attr_t = -1;
+        if (attr_t != dev) {
+            cudaError_t e = cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM);
+            if (e != cudaSuccess) return e;
+            attr_t = dev;
+        }
+        kt<<<grid, WF64_NT, SH::SMEM, s>>>(tin, tsrc, out, a.g, cf, a.res, iter0, a.tol, a.sc, chunk);
+        return cudaGetLastError();
+    }
     kern<<<grid, WF64_NT, sm, s>>>(in, out, a.rho, a.g, cf, a.res, iter0, a.tol, a.sc, chunk);
     return cudaGetLastError();
 }

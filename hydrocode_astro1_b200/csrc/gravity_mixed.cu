@@ -372,8 +372,11 @@ cudaError_t mixed_check(const GravArgs &a, int iter, double thresh, cudaStream_t
 // FP32 correction sweeps with temporal blocking: 4 iterations per HBM pass.
 // ---------------------------------------------------------------------------
 #include "sor_wavefront.cuh"
+#include "sor_wavefront_tma.cuh"
+#include "tmap.cuh"
 
 namespace hc {
+bool wf_tma_enabled();
 namespace {
 constexpr int WF32_TJ = 16, WF32_TK = 64, WF32_NT = 512;
 template <int TT>
@@ -405,6 +408,21 @@ cudaError_t pass32(const GravArgs &a, const float *in, float *out, const float *
     int chunk = (nint + chunks - 1) / chunks;
     chunks = (nint + chunk - 1) / chunk;
     dim3 grid(tk, tj, chunks);
+    using SH = wtma::Shape<float, TT, WF32_TJ, WF32_TK>;
+    CUtensorMap tin, tsrc;
+    // FP32 bulk copies start on 16 bytes: k0 - 2T must be a multiple of 4
+    if (TT >= 2 && wf_tma_enabled() && tmap3(in, 4, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tin) &&
+        tmap3(r32, 4, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tsrc)) {
+        auto kt = wtma::sor_wavefront_tma_kernel<float, float, TT, WF32_TJ, WF32_TK, WF32_NT>;
+        static int attr_t = -1;
+        if (attr_t != dev) {
+            cudaError_t e = cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM);
+            if (e != cudaSuccess) return e;
+            attr_t = dev;
+        }
+        kt<<<grid, WF32_NT, SH::SMEM, s>>>(tin, tsrc, out, a.g, cf, a.res, iter0, thresh, a.sc, chunk);
+        return cudaGetLastError();
+    }
     kern<<<grid, WF32_NT, sm, s>>>(in, out, r32, a.g, cf, a.res, iter0, thresh, a.sc, chunk);
     return cudaGetLastError();
 }

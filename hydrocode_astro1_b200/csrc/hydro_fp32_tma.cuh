@@ -54,7 +54,6 @@ __device__ __forceinline__ Rec make_rec(float d, float mx, float my, float mz, f
 }
 
 template <int A> __device__ __forceinline__ float vel(const Rec &r) { return A == 0 ? r.b.y : (A == 1 ? r.b.z : r.b.w); }
-template <int A> __device__ __forceinline__ float mom(const Rec &r) { return A == 0 ? r.a.y : (A == 1 ? r.a.z : r.a.w); }
 
 // HLLC flux along axis A (hydro_solver_3d.c:239-300), branch-free side choice
 template <int A>
@@ -70,25 +69,30 @@ __device__ __forceinline__ Flux hllc(const Rec &L, const Rec &R)
     const bool supl = sL >= 0.f;
     const bool supr = !supl && (sR <= 0.f);
     const bool left = supl || (!supr && ss >= 0.f);
-    const Rec &K = left ? L : R;
+    // Select the upwind side value by value: a reference bound to one of two
+    // register-resident records (the x faces) gave wrong conserved
+    // components on sm_100a, selects do not.
     const float sK = left ? sL : sR;
-    const float uK = vel<A>(K), dK = K.c.z, pK = K.c.x, iK = K.c.w;
-    const float EK = K.b.x;
+    const float uK = left ? uL : uR, dK = left ? dL : dR, pK = left ? pL : pR;
+    const float iK = left ? L.c.w : R.c.w, EK = left ? L.b.x : R.b.x;
+    const float qd = left ? L.a.x : R.a.x, q0 = left ? L.a.y : R.a.y;
+    const float q1 = left ? L.a.z : R.a.z, q2 = left ? L.a.w : R.a.w;
+    const float v0 = left ? L.b.y : R.b.y, v1 = left ? L.b.z : R.b.z, v2 = left ? L.b.w : R.b.w;
     // F(U_K)
     Flux f;
-    f.d = mom<A>(K);
-    f.m0 = K.a.y * uK + (A == 0 ? pK : 0.f);
-    f.m1 = K.a.z * uK + (A == 1 ? pK : 0.f);
-    f.m2 = K.a.w * uK + (A == 2 ? pK : 0.f);
+    f.d = A == 0 ? q0 : (A == 1 ? q1 : q2);
+    f.m0 = q0 * uK + (A == 0 ? pK : 0.f);
+    f.m1 = q1 * uK + (A == 1 ? pK : 0.f);
+    f.m2 = q2 * uK + (A == 2 ? pK : 0.f);
     f.e = (EK + pK) * uK;
     if (!(supl || supr)) {
         const float fac = __fdividef(sK - uK, sK - ss);
         const float sd = dK * fac;
         const float se = sd * (EK * iK + (ss - uK) * (ss + __fdividef(pK * iK, sK - uK)));
-        f.d += sK * (sd - K.a.x);
-        f.m0 += sK * (sd * (A == 0 ? ss : K.b.y) - K.a.y);
-        f.m1 += sK * (sd * (A == 1 ? ss : K.b.z) - K.a.z);
-        f.m2 += sK * (sd * (A == 2 ? ss : K.b.w) - K.a.w);
+        f.d += sK * (sd - qd);
+        f.m0 += sK * (sd * (A == 0 ? ss : v0) - q0);
+        f.m1 += sK * (sd * (A == 1 ? ss : v1) - q1);
+        f.m2 += sK * (sd * (A == 2 ? ss : v2) - q2);
         f.e += sK * (se - EK);
     }
     return f;
