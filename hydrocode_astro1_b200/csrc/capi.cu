@@ -72,6 +72,7 @@ struct hc_ctx {
     int cfl_valid;
     // gravity
     double *phi, *phig, *rho_ext, *phi2;
+    double *phs, *rhs;           // colour-split potential and density (FP64 solve)
     float *e32, *r32, *e32b;     // mixed precision correction (ping-pong) / residual
     double *gx, *gy, *gz;
     double *res;
@@ -140,10 +141,19 @@ static void resolve_timers(hc_ctx *c)
     c->pend.clear();
 }
 
+// Waits for the context's stream and reports the sticky device error code
+// (set by a kernel whose bounded wait ran out), clearing it.
 static int sync_ctx(hc_ctx *c)
 {
+    CK(cudaMemcpyAsync(&c->hsc->err, &c->sc->err, sizeof(int), cudaMemcpyDeviceToHost, c->s));
     CK(cudaStreamSynchronize(c->s));
     resolve_timers(c);
+    if (c->hsc->err) {
+        const int e = c->hsc->err;
+        c->hsc->err = 0;
+        CK(cudaMemsetAsync(&c->sc->err, 0, sizeof(int), c->s));
+        return set_err(e, "a bounded wait in a device kernel gave up");
+    }
     return HC_OK;
 }
 
@@ -179,6 +189,7 @@ static void free_ctx(hc_ctx *c)
             if (c->q32[b][v] && v == 0) cudaFree(c->q32[b][0]);
         }
     cudaFree(c->phi); cudaFree(c->phig); cudaFree(c->rho_ext); cudaFree(c->phi2);
+    cudaFree(c->phs); cudaFree(c->rhs);
     cudaFree(c->e32); cudaFree(c->r32); cudaFree(c->e32b);
     cudaFree(c->gx); cudaFree(c->gy); cudaFree(c->gz);
     cudaFree(c->res); cudaFree(c->scratch); cudaFree(c->mom);
@@ -299,9 +310,11 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
         if (!rc) rc = dmalloc((void **)&c->scratch, c->scratch_len * sizeof(double));
         if (!rc) rc = dmalloc((void **)&c->mom, 4 * 1024 * sizeof(double));
         if (!rc && k.precision == HC_FP32) {
-            rc = dmalloc((void **)&c->e32, n * sizeof(float));
-            if (!rc) rc = dmalloc((void **)&c->r32, n * sizeof(float));
-            if (!rc) rc = dmalloc((void **)&c->e32b, n * sizeof(float));
+            // sized for the colour-split layout (>= n cells)
+            const size_t ns = (size_t)std::max<long long>(split_len(c->g), (long long)n);
+            rc = dmalloc((void **)&c->e32, ns * sizeof(float));
+            if (!rc) rc = dmalloc((void **)&c->r32, ns * sizeof(float));
+            if (!rc) rc = dmalloc((void **)&c->e32b, ns * sizeof(float));
         }
     }
     if (!rc && cudaMallocHost((void **)&c->hsc, sizeof(DevScalars)) != cudaSuccess)
@@ -314,8 +327,9 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
         if (c->q32[b][0]) cudaMemsetAsync(c->q32[b][0], 0, 5 * n * sizeof(float), c->s);
     }
     if (c->e32b) {
-        cudaMemsetAsync(c->e32, 0, n * sizeof(float), c->s);
-        cudaMemsetAsync(c->e32b, 0, n * sizeof(float), c->s);
+        const size_t ns = (size_t)std::max<long long>(split_len(c->g), (long long)n);
+        cudaMemsetAsync(c->e32, 0, ns * sizeof(float), c->s);
+        cudaMemsetAsync(c->e32b, 0, ns * sizeof(float), c->s);
     }
     if (c->phi) {
         cudaMemsetAsync(c->phi, 0, n * sizeof(double), c->s);
@@ -505,11 +519,22 @@ static int sor_fp64(hc_ctx *c, const double *rho)
         c->diag.last_residual = 0.0;
         return -1;
     }
-    // sor_depth -1: one kernel per colour, in place (the reference's sweeps);
-    // otherwise one wavefront pass per iteration, out of place between
-    // phi (buf 0) and phi2 (buf 1): iteration t reads buf[t%2], writes buf[(t+1)%2]
-    const bool wave = c->cfg.sor_depth >= 0 && c->g.nz >= 3;
+    // sor_depth 0 (default): colour-split sweeps, in place on a split copy of
+    // phi and rho; -1: one kernel per colour on the natural layout, in place
+    // (the reference's sweeps); >= 1: one wavefront pass per iteration, out of
+    // place between phi (buf 0) and phi2 (buf 1): iteration t reads buf[t%2],
+    // writes buf[(t+1)%2].  All three give the same iterates.
+    const bool split = c->cfg.sor_depth == 0 && c->g.nz >= 3;
+    const bool wave = c->cfg.sor_depth >= 1 && c->g.nz >= 3;
     double *buf[2] = { c->phi, c->phi2 };
+    if (split) {
+        const size_t ns = (size_t)split_len(c->g);
+        if (!c->phs) rc = dmalloc((void **)&c->phs, ns * sizeof(double));
+        if (!rc && !c->rhs) rc = dmalloc((void **)&c->rhs, ns * sizeof(double));
+        if (rc) return rc;
+        CK(grav_split_fields(a, c->phs, c->rhs, c->s));
+        c->launches += 2;
+    }
     if (wave) {
         if (!c->phi2) {
             rc = dmalloc((void **)&c->phi2, (size_t)c->g.n * sizeof(double));
@@ -520,7 +545,12 @@ static int sor_fp64(hc_ctx *c, const double *rho)
         CK(cudaMemcpyAsync(c->phi2, c->phi, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
     }
     auto one_iter = [&](int q) -> int {
-        if (wave) {
+        if (split) {
+            CK(grav_sor_split(a, c->phs, c->rhs, 0, q, c->s));
+            CK(grav_sor_split(a, c->phs, c->rhs, 1, q, c->s));
+            c->launches += 2;
+            c->sor_launches += 2;
+        } else if (wave) {
             CK(grav_sor_pass64(a, buf[q & 1], buf[(q + 1) & 1], q, c->s));
             c->launches += 1;
             c->sor_launches += 1;
@@ -546,6 +576,10 @@ static int sor_fp64(hc_ctx *c, const double *rho)
     }
     rc = grav_boundary_values(c, a);
     if (rc) return rc;
+    if (split) {
+        CK(grav_split_boundary(a, c->phs, c->s));
+        c->launches += 1;
+    }
     int it = 1, done = 0, last = 0;
     int batch = 16;
     while (true) {
@@ -570,6 +604,10 @@ static int sor_fp64(hc_ctx *c, const double *rho)
     }
     int used = done ? last : a.max_iter;
     if (wave && (used & 1)) std::swap(c->phi, c->phi2);   // result in buf[used % 2]
+    if (split) {
+        CK(grav_unsplit(a, c->phs, c->s));
+        c->launches += 1;
+    }
     double rv = 0.0;
     CK(cudaMemcpy(&rv, c->res + (used - 1), sizeof(double), cudaMemcpyDeviceToHost));
     c->diag.last_iterations = used;
@@ -585,6 +623,11 @@ static int sor_fp64(hc_ctx *c, const double *rho)
 int hc_sor_mixed(hc_ctx *c, const float *rho32)
 {
     GravArgs a = grav_args(c, nullptr, rho32);
+    // sor_depth 0 (default): colour-split sweeps on e and r; -1: one in-place
+    // kernel per colour on the natural layout; >= 1: wavefront passes of that
+    // many FP32 iterations per HBM pass (temporal blocking)
+    const bool split = c->cfg.sor_depth == 0 && c->g.nz >= 3;
+    const int depth = c->cfg.sor_depth == 0 ? -1 : c->cfg.sor_depth;
     int rc = ensure_res(c, a.max_iter);
     if (rc) return rc;
     a.res = c->res;
@@ -598,7 +641,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         {
             FamTimer t(c, FAM_RES);
             CK(cudaMemsetAsync(&c->sc->resnorm, 0, sizeof(double), c->s));
-            CK(mixed_residual(a, c->r32, c->e32, c->s));
+            CK(mixed_residual(a, c->r32, c->e32, split, c->s));
             c->launches++;
         }
         CK(cudaMemcpyAsync(&c->hsc->resnorm, &c->sc->resnorm, sizeof(double), cudaMemcpyDeviceToHost, c->s));
@@ -619,14 +662,13 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         }
         // one cycle reduces the residual 1e4-fold at most: FP32 resolves the
         // correction e to ~1e-7 |e|, and |e| can exceed max|delta| by the
-        // grid's condition number on a cold start
-        const double thresh = std::max(0.5 * a.tol, 1.0e-4 * dmax);
+        // grid's condition number on a cold start.  In the last cycle the
+        // sweeps run to the reference's own test: a red-black sweep whose
+        // update norm max |phi_GS - phi_old| is below tol.
+        const double thresh = std::max(a.tol, 1.0e-4 * dmax);
         const int budget = a.max_iter - total;
         CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));
         CK(grav_reset_slots(a, 0, budget + 8, c->s));
-        // depth: FP32 iterations per HBM pass (temporal blocking); -1 selects
-        // one in-place kernel per colour
-        const int depth = c->cfg.sor_depth == 0 ? 4 : c->cfg.sor_depth;
         float *eb[2] = { c->e32, c->e32b };
         int it = 0, done = 0, last = 0, batch = 16, processed = 0, best_it = 0;
         double best = 1e300;
@@ -636,7 +678,14 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
             int end = std::min(budget, it + batch);
             {
                 FamTimer t(c, FAM_SOR);
-                if (depth < 0) {
+                if (split) {
+                    for (int q = it; q < end; q++) {
+                        CK(mixed_sor32_split(a, c->e32, c->r32, 0, q, thresh, c->s));
+                        CK(mixed_sor32_split(a, c->e32, c->r32, 1, q, thresh, c->s));
+                    }
+                    c->launches += 2 * (end - it);
+                    c->sor_launches += 2 * (end - it);
+                } else if (depth < 0) {
                     for (int q = it; q < end; q++) {
                         CK(mixed_sor32(a, c->e32, c->r32, 0, q, thresh, c->s));
                         CK(mixed_sor32(a, c->e32, c->r32, 1, q, thresh, c->s));
@@ -681,11 +730,36 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         const int used = done ? last : processed;
         total += used;
         // the correction is in eb[passes % 2] for the blocked sweeps
-        const float *efinal = (depth < 0) ? c->e32 : eb[(used / depth) & 1];
+        const float *efinal = (split || depth < 0) ? c->e32 : eb[(used / depth) & 1];
         {
             FamTimer t(c, FAM_RES);
-            CK(mixed_update(a, efinal, c->s));
+            CK(cudaMemsetAsync(&c->sc->resid_bits, 0, sizeof(unsigned long long), c->s));
+            CK(mixed_update(a, efinal, split, c->s));
             c->launches++;
+        }
+        // Converged by the reference's criterion when the last sweep's update
+        // norm (on e, which equals that of phi + e) is below tol and FP32
+        // resolves e finely enough that an update of size tol cannot round
+        // away: max|e| 2^-22 < tol.
+        if (done && thresh == a.tol) {
+            double snorm = 0.0;
+            CK(cudaMemcpyAsync(&c->hsc->resnorm, c->res + (last - 1), sizeof(double), cudaMemcpyDeviceToHost,
+                               c->s));
+            CK(cudaMemcpyAsync(&c->hsc->resid_bits, &c->sc->resid_bits, sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, c->s));
+            rc = sync_ctx(c);
+            if (rc) return rc;
+            snorm = c->hsc->resnorm;
+            double emax;
+            memcpy(&emax, &c->hsc->resid_bits, sizeof emax);
+            if (c->debug)
+                fprintf(stderr, "[hc] mixed cycle %d: sweep norm %.3e, max|e| %.3e after %d sweeps\n", cycles, snorm,
+                        emax, total);
+            if (snorm < a.tol && emax * 0x1p-22 < a.tol) {
+                dmax = snorm;
+                status = 0;
+                break;
+            }
         }
     }
     c->diag.last_iterations = total;

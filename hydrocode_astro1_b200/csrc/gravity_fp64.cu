@@ -581,3 +581,55 @@ cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, in
 }
 
 }  // namespace hc
+
+// ---------------------------------------------------------------------------
+// Colour-split SOR (the default FP64 solve for nz >= 3)
+// ---------------------------------------------------------------------------
+#include "sor_split.cuh"
+
+namespace hc {
+
+long long split_len(const Geom &g)
+{
+    const Split sp = make_split(g);
+    return 2 * sp.cs;
+}
+
+cudaError_t grav_split_fields(const GravArgs &a, double *phs, double *rhs, cudaStream_t s)
+{
+    const Split sp = make_split(a.g);
+    const unsigned rows = (unsigned)((long long)a.g.nx * a.g.ny);
+    const int nt = a.g.nz >= 256 ? 256 : 128;
+    split_copy_kernel<double, double><<<rows, nt, 0, s>>>(a.phi, phs, sp);
+    if (rhs) split_copy_kernel<double, double><<<rows, nt, 0, s>>>(a.rho, rhs, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t grav_split_boundary(const GravArgs &a, double *phs, cudaStream_t s)
+{
+    const Split sp = make_split(a.g);
+    split_boundary_kernel<double><<<148 * 4, 256, 0, s>>>(a.phi, phs, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t grav_unsplit(const GravArgs &a, const double *phs, cudaStream_t s)
+{
+    const Split sp = make_split(a.g);
+    const unsigned rows = (unsigned)((long long)a.g.nx * a.g.ny);
+    unsplit_copy_kernel<double><<<rows, a.g.nz >= 256 ? 256 : 128, 0, s>>>(phs, a.phi, sp);
+    return cudaGetLastError();
+}
+
+cudaError_t grav_sor_split(const GravArgs &a, double *phs, const double *rhs, int colour, int iter, cudaStream_t s)
+{
+    SorCoef<double> cf;
+    cf.ix2 = 1.0 / (a.g.dx * a.g.dx);
+    cf.iy2 = 1.0 / (a.g.dy * a.g.dy);
+    cf.iz2 = 1.0 / (a.g.dz * a.g.dz);
+    cf.fpg = 4.0 * M_PI * a.G;
+    cf.fac = 2.0 * (cf.ix2 + cf.iy2 + cf.iz2);
+    cf.om = a.omega;
+    return launch_sor_split<double, double>(phs, rhs, make_split(a.g), cf, colour, a.res, iter, a.tol, a.sc, s);
+}
+
+}  // namespace hc

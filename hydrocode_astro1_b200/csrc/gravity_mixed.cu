@@ -15,6 +15,7 @@
 
 #include "hc_internal.cuh"
 #include "hc_math.cuh"
+#include "sor_split.cuh"
 
 namespace hc {
 
@@ -232,7 +233,7 @@ struct MixConst {
     float cx, cy, cz, om;
 };
 
-__device__ __forceinline__ MixConst mix_const(const GravArgs &a)
+__host__ __device__ __forceinline__ MixConst mix_const(const GravArgs &a)
 {
     MixConst c;
     c.ix2 = 1.0 / (a.g.dx * a.g.dx);
@@ -262,7 +263,8 @@ __device__ __forceinline__ double block_max_any(double v)
     return m;
 }
 
-__global__ void __launch_bounds__(256) mixed_residual_kernel(GravArgs a, float *r32, float *e32)
+// r32 / e32 in the natural layout, or colour-split (sp.cs > 0)
+__global__ void __launch_bounds__(256) mixed_residual_kernel(GravArgs a, float *r32, float *e32, Split sp)
 {
     const Geom g = a.g;
     const MixConst mc = mix_const(a);
@@ -271,6 +273,7 @@ __global__ void __launch_bounds__(256) mixed_residual_kernel(GravArgs a, float *
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
          c += (long long)gridDim.x * blockDim.x) {
         int i = (int)(c / sI), j = (int)((c / sJ) % g.ny), k = (int)(c % sJ);
+        const long long o = sp.cs ? sp.at(i, j, k) : c;
         float d = 0.f;
         if (i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2) {
             const double *phi = a.phi;
@@ -281,18 +284,28 @@ __global__ void __launch_bounds__(256) mixed_residual_kernel(GravArgs a, float *
             m = tmax(m, fabs(dd));
             d = (float)dd;
         }
-        r32[c] = d;
-        e32[c] = 0.f;
+        r32[o] = d;
+        e32[o] = 0.f;
     }
     double b = block_max_any<256>(m);
     if (threadIdx.x == 0) atomic_max_nonneg((unsigned long long *)&a.sc->resnorm, b);
 }
 
-__global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const float *e32)
+// phi += e; max|e| into sc->resid_bits (the FP32 resolution check)
+__global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const float *e32, Split sp)
 {
+    const long long sI = (long long)a.g.ny * a.g.nz, sJ = a.g.nz;
+    float m = 0.f;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < a.g.n;
-         c += (long long)gridDim.x * blockDim.x)
-        a.phi[c] += (double)e32[c];
+         c += (long long)gridDim.x * blockDim.x) {
+        long long o = c;
+        if (sp.cs) o = sp.at((int)(c / sI), (int)((c / sJ) % a.g.ny), (int)(c % sJ));
+        const float e = e32[o];
+        a.phi[c] += (double)e;
+        m = tmax(m, fabsf(e));
+    }
+    const double b = block_max_any<256>((double)m);
+    if (threadIdx.x == 0 && b > 0.0) atomic_max_nonneg(&a.sc->resid_bits, b);
 }
 
 constexpr int S32_BX = 32, S32_BY = 8;
@@ -339,16 +352,35 @@ __global__ void check32_kernel(GravArgs a, int iter, double thresh)
 
 }  // namespace
 
-cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, cudaStream_t s)
+static Split split_or_natural(const GravArgs &a, bool split)
 {
-    mixed_residual_kernel<<<148 * 8, 256, 0, s>>>(a, r32, e32);
+    Split sp = make_split(a.g);
+    if (!split) sp.cs = 0;
+    return sp;
+}
+
+cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, bool split, cudaStream_t s)
+{
+    mixed_residual_kernel<<<148 * 8, 256, 0, s>>>(a, r32, e32, split_or_natural(a, split));
     return cudaGetLastError();
 }
 
-cudaError_t mixed_update(const GravArgs &a, const float *e32, cudaStream_t s)
+cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, cudaStream_t s)
 {
-    mixed_update_kernel<<<148 * 8, 256, 0, s>>>(a, e32);
+    mixed_update_kernel<<<148 * 8, 256, 0, s>>>(a, e32, split_or_natural(a, split));
     return cudaGetLastError();
+}
+
+cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, int colour, int iter,
+                              double thresh, cudaStream_t s)
+{
+    const MixConst mc = mix_const(a);
+    SorCoef<float> cf;
+    cf.cx = mc.cx;
+    cf.cy = mc.cy;
+    cf.cz = mc.cz;
+    cf.om = mc.om;
+    return launch_sor_split<float, float>(e32, r32, make_split(a.g), cf, colour, a.res, iter, thresh, a.sc, s);
 }
 
 cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int color, int iter,

@@ -155,8 +155,11 @@ int lmax_ncoef(int lmax);
 }  // namespace hc
 
 namespace hc {
-cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, cudaStream_t s);
-cudaError_t mixed_update(const GravArgs &a, const float *e32, cudaStream_t s);
+// split: r32 / e32 in the colour-split layout of sor_split.cuh
+cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, bool split, cudaStream_t s);
+cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, cudaStream_t s);
+cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, int colour, int iter,
+                              double thresh, cudaStream_t s);
 cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int color, int iter,
                         double thresh, cudaStream_t s);
 cudaError_t mixed_check(const GravArgs &a, int iter, double thresh, cudaStream_t s);
@@ -164,6 +167,14 @@ cudaError_t mixed_check(const GravArgs &a, int iter, double thresh, cudaStream_t
 
 namespace hc {
 cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, int iter0, cudaStream_t s);
+// colour-split FP64 SOR (sor_split.cuh): elements of a split field, natural
+// -> split copies of phi (and rho), boundary cells only, split -> natural phi,
+// one colour sweep
+long long split_len(const Geom &g);
+cudaError_t grav_split_fields(const GravArgs &a, double *phs, double *rhs, cudaStream_t s);
+cudaError_t grav_split_boundary(const GravArgs &a, double *phs, cudaStream_t s);
+cudaError_t grav_unsplit(const GravArgs &a, const double *phs, cudaStream_t s);
+cudaError_t grav_sor_split(const GravArgs &a, double *phs, const double *rhs, int colour, int iter, cudaStream_t s);
 cudaError_t mixed_sor32_pass(const GravArgs &a, const float *in, float *out, const float *r32, int iter0,
                              int depth, double thresh, cudaStream_t s);
 }  // namespace hc

@@ -1,0 +1,184 @@
+// sor_split.cuh -- red-black SOR sweeps on a colour-split layout.
+//
+// The red and the black cells of a field are stored in two separate arrays,
+// each a dense (i, j, m) block: cell (i, j, k) has colour c = (i+j+k) & 1 and
+// lives at  c*cs + (i*ny + j)*H + (k >> 1),  H = (nz+1)/2,  cs = nx*ny*H.
+// A colour sweep then reads the other colour's array, its own array and the
+// source (all unit-stride along m) and writes its own array with full-sector
+// stores: 4 x 1/2 x sizeof(T) bytes per cell per colour, no stride-2 access
+// and no partially written sectors.
+//
+// Neighbours of a cell of colour c at (i, j, m) with k = 2m + s,
+// s = (i + j + c) & 1, are all of the other colour:
+//   x+-1, y+-1 : same m in the rows (i+-1, j) and (i, j+-1)
+//   z-1 / z+1  : m-1 / m (s = 0) or m / m+1 (s = 1) in row (i, j)
+// Each thread updates one (j, m) column over a few planes, loading all their
+// operands before the first update.  Within a colour the updates are
+// independent, so the iterates are those of the reference's sweep
+// (gravity_solver_3d.c:566-728) bit for bit in FP64 (same operand order,
+// SorCoef<double>).
+//
+// The update norm max |phi_GS - phi_old| of the sweep is reduced per CTA
+// into the iteration's slot with one atomic.  A red sweep whose previous
+// iteration's slot is already below the stop threshold sets the done flag
+// instead of sweeping; every later sweep of the batch then returns at once.
+#pragma once
+#include "hc_internal.cuh"
+#include "hc_math.cuh"
+#include "sor_wavefront.cuh"
+
+namespace hc {
+
+struct Split {
+    int nx, ny, nz, H;
+    long long cs;   // elements per colour
+    __host__ __device__ __forceinline__ long long at(int i, int j, int k) const
+    {
+        return (long long)((i + j + k) & 1) * cs + ((long long)i * ny + j) * H + (k >> 1);
+    }
+};
+
+inline Split make_split(const Geom &g)
+{
+    Split s;
+    s.nx = g.nx;
+    s.ny = g.ny;
+    s.nz = g.nz;
+    s.H = (g.nz + 1) / 2;
+    s.cs = (long long)g.nx * g.ny * s.H;
+    return s;
+}
+
+constexpr int SPLIT_BX = 32, SPLIT_BY = 8;
+
+// One thread owns the column (j, m) over NI consecutive planes i0..i0+NI-1:
+// every operand of the NI updates is loaded first (6 NI + 2 independent
+// loads in flight per thread), then the updates run and are stored.
+template <typename T, typename S, int NI>
+__global__ void __launch_bounds__(SPLIT_BX * SPLIT_BY)
+sor_split_kernel(T *__restrict__ own, const T *__restrict__ oth, const S *__restrict__ src, Split sp,
+                 SorCoef<T> cf, int colour, double *res, int iter, double thresh, DevScalars *sc)
+{
+    __shared__ double wmax[SPLIT_BX * SPLIT_BY / 32];
+    if (*(volatile int *)&sc->done) return;
+    if (colour == 0 && iter > 0) {
+        const double prev = __longlong_as_double(*reinterpret_cast<const volatile long long *>(res + iter - 1));
+        if (prev < thresh) {
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                sc->last_iter = iter;
+                sc->done = 1;
+            }
+            return;
+        }
+    }
+    const int m = blockIdx.x * SPLIT_BX + threadIdx.x;
+    const int j = blockIdx.y * SPLIT_BY + threadIdx.y;
+    const int i0 = 1 + blockIdx.z * NI;
+    T rmax = (T)0;
+    if (j >= 1 && j <= sp.ny - 2 && m < sp.H) {
+        const long long sJ = sp.H, sI = (long long)sp.ny * sp.H;
+        const long long o0 = (long long)i0 * sI + (long long)j * sJ + m;
+        const int ilast = sp.nx - 2;                 // last interior plane
+        // x column: planes i0-1 .. i0+NI, clamped to the grid
+        T x[NI + 2];
+#pragma unroll
+        for (int q = 0; q < NI + 2; q++) {
+            const int i = min(i0 - 1 + q, ilast + 1);
+            x[q] = oth[o0 + (long long)(i - i0) * sI];
+        }
+        T ym[NI], yp[NI], zo[NI], ow[NI];
+        S sr[NI];
+#pragma unroll
+        for (int q = 0; q < NI; q++) {
+            const int i = min(i0 + q, ilast);
+            const long long o = o0 + (long long)(i - i0) * sI;
+            const long long row = o - m;             // first element of row (i, j)
+            const int s = (i + j + colour) & 1;
+            ym[q] = oth[o - sJ];
+            yp[q] = oth[o + sJ];
+            // the z neighbour that is not in this column: m-1 (s = 0) or m+1
+            // (s = 1), clamped to the row (only interior cells use it)
+            zo[q] = oth[s ? min(o + 1, row + sp.H - 1) : max(o - 1, row)];
+            ow[q] = own[o];
+            sr[q] = src[o];
+        }
+#pragma unroll
+        for (int q = 0; q < NI; q++) {
+            const int i = i0 + q;
+            const int s = (i + j + colour) & 1;
+            const int k = 2 * m + s;
+            if (i <= ilast && k >= 1 && k <= sp.nz - 2) {
+                const T zm = s ? x[q + 1] : zo[q];
+                const T zp = s ? zo[q] : x[q + 1];
+                T r;
+                own[o0 + (long long)q * sI] =
+                    cf.update(ow[q], x[q], x[q + 2], ym[q], yp[q], zm, zp, (T)sr[q], r);
+                rmax = tmax(rmax, r);
+            }
+        }
+    }
+    double v = (double)rmax;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = tmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+    const int tid = threadIdx.y * SPLIT_BX + threadIdx.x;
+    if ((tid & 31) == 0) wmax[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        double b = 0.0;
+#pragma unroll
+        for (int w = 0; w < SPLIT_BX * SPLIT_BY / 32; w++) b = tmax(b, wmax[w]);
+        // most CTAs find the slot already at or above their value
+        unsigned long long *slot = (unsigned long long *)(res + iter);
+        if (b > 0.0 && (unsigned long long)__double_as_longlong(b) > *(volatile unsigned long long *)slot)
+            atomic_max_nonneg(slot, b);
+    }
+}
+
+// natural (k fastest) -> colour-split copy; one CTA per row (i, j)
+template <typename A, typename B>
+__global__ void split_copy_kernel(const A *__restrict__ nat, B *__restrict__ spl, Split sp)
+{
+    const long long row = blockIdx.x;   // i*ny + j
+    const int i = (int)(row / sp.ny), j = (int)(row % sp.ny);
+    const A *r = nat + row * sp.nz;
+    for (int k = threadIdx.x; k < sp.nz; k += blockDim.x) spl[sp.at(i, j, k)] = (B)r[k];
+}
+
+// colour-split -> natural copy; one CTA per row (i, j)
+template <typename T>
+__global__ void unsplit_copy_kernel(const T *__restrict__ spl, T *__restrict__ nat, Split sp)
+{
+    const long long row = blockIdx.x;
+    const int i = (int)(row / sp.ny), j = (int)(row % sp.ny);
+    T *r = nat + row * sp.nz;
+    for (int k = threadIdx.x; k < sp.nz; k += blockDim.x) r[k] = spl[sp.at(i, j, k)];
+}
+
+// boundary cells only (the Dirichlet values of the solve)
+template <typename T>
+__global__ void split_boundary_kernel(const T *__restrict__ nat, T *__restrict__ spl, Split sp)
+{
+    const long long nb = boundary_count(sp.nx, sp.ny, sp.nz, true);
+    const long long sI = (long long)sp.ny * sp.nz, sJ = sp.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        boundary_cell(t, sp.nx, sp.ny, sp.nz, true, i, j, k);
+        spl[sp.at(i, j, k)] = nat[i * sI + j * sJ + k];
+    }
+}
+
+template <typename T, typename S>
+cudaError_t launch_sor_split(T *base, const S *src, const Split &sp, const SorCoef<T> &cf, int colour,
+                             double *res, int iter, double thresh, DevScalars *sc, cudaStream_t s)
+{
+    constexpr int NI = sizeof(T) == 8 ? 2 : 4;
+    dim3 grid((sp.H + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + NI - 1) / NI);
+    T *own = base + (size_t)colour * sp.cs;
+    const T *oth = base + (size_t)(colour ^ 1) * sp.cs;
+    sor_split_kernel<T, S, NI><<<grid, dim3(SPLIT_BX, SPLIT_BY), 0, s>>>(own, oth, src + (size_t)colour * sp.cs, sp,
+                                                                         cf, colour, res, iter, thresh, sc);
+    return cudaGetLastError();
+}
+
+}  // namespace hc

@@ -126,6 +126,10 @@ sor_wavefront_tma_kernel(const __grid_constant__ CUtensorMap tm_in, const __grid
     // (L0-1) and (L0+1) share a barrier: wait before its next use
     ok = bar_wait(&bar[(L0 - 1) & 1], phase[(L0 - 1) & 1]) && ok;
     phase[(L0 - 1) & 1] ^= 1u;
+    // every thread must have observed that phase before the barrier is armed
+    // again: a thread still polling parity 0 after the next phase completed
+    // would wait for the phase after that
+    __syncthreads();
     issue(L0 + 1, true, L0, false, 0);         // potential plane L0 on bar[(L0+1)&1]
     ok = bar_wait(&bar[(L0 + 1) & 1], phase[(L0 + 1) & 1]) && ok;
     phase[(L0 + 1) & 1] ^= 1u;

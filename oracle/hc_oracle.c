@@ -550,6 +550,26 @@ double hco_residual_norm(const hco_grid *g, const double *phi, const double *rho
     return res;
 }
 
+/* The convergence test of gravity_solve_potential (gravity_solver_3d.c:
+ * 702-714) applied to a given potential: the update norm max |phi_GS -
+ * phi_old| of one red-black sweep started from phi (phi is not changed). */
+double hco_sweep_norm(hco_grid *g, const double *phi, const double *rho)
+{
+    double ix2, iy2, iz2;
+    double fac = sor_factor(g, &ix2, &iy2, &iz2);
+    double fpg = 4.0 * M_PI * g->G;
+    const size_t n = (size_t)g->nx * g->ny * g->nz;
+    double *work = (double *)malloc(n * sizeof(double));
+    memcpy(work, phi, n * sizeof(double));
+    double *keep = g->phi;
+    g->phi = work;
+    double r0 = sor_color(g, rho, 0, ix2, iy2, iz2, fpg, fac);
+    double r1 = sor_color(g, rho, 1, ix2, iy2, iz2, fpg, fac);
+    g->phi = keep;
+    free(work);
+    return mx(mx(0.0, r0), r1);
+}
+
 /* ------------------------------------------------------------------------ */
 /* The time step                                                             */
 /* ------------------------------------------------------------------------ */

@@ -69,6 +69,7 @@ void hco_boundary_lmax(hco_grid *g, int lmax, const double *com, const double *c
  * |(lap_nbrs(phi) - 4 pi G rho)/factor - phi|, the quantity the reference's
  * update norm measures when evaluated at a fixed phi. */
 double hco_residual_norm(const hco_grid *g, const double *phi, const double *rho);
+double hco_sweep_norm(hco_grid *g, const double *phi, const double *rho);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,8 @@ def oracle_lib():
         lib.hco_boundary_lmax.argtypes = [gp, C.c_int, _dp, _dp]
         lib.hco_residual_norm.argtypes = [gp, _dp, _dp]
         lib.hco_residual_norm.restype = C.c_double
+        lib.hco_sweep_norm.argtypes = [gp, _dp, _dp]
+        lib.hco_sweep_norm.restype = C.c_double
         _olib = lib
     return _olib
 
@@ -159,6 +161,12 @@ class OracleSim:
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         rho = np.ascontiguousarray(rho, dtype=np.float64)
         return self.lib.hco_residual_norm(C.byref(self.g), _ptr(phi), _ptr(rho))
+
+    def sweep_norm(self, phi, rho):
+        """Update norm of one red-black sweep from phi: the reference's test."""
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        return self.lib.hco_sweep_norm(C.byref(self.g), _ptr(phi), _ptr(rho))
 
 
 def have_reference():
