@@ -167,12 +167,15 @@ def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
         warm_iters.append(s.diagnostics()["last_iterations"])
         log(f"[bench] {variant} warm-up step {w}: {time.perf_counter() - t:.3f} s, "
             f"{warm_iters[-1]} SOR iterations")
-    s.timing(reset=True)
+    warm_launches = s.timing(reset=True)["launches"]
     iters = []
     barrier(dist)
     s.sync()
     if clocks:
         clocks.start()
+    nvtx = nvtx_mod()
+    if nvtx:
+        nvtx.range_push("timed")     # lets `ncu --nvtx --nvtx-include timed/` list the timed launches
     s.timer_start()
     dts = []
     d0 = s.diagnostics()["total_iterations"]
@@ -180,12 +183,22 @@ def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
         dts.append(float(s.step(1)[0]))
         iters.append(s.diagnostics()["last_iterations"])
     ms = s.timer_stop()
+    if nvtx:
+        nvtx.range_pop()
     ck = clocks.stop() if clocks else None
     log(f"[bench] {variant}: {steps} timed steps {ms:.1f} ms, SOR iterations {iters}")
     tm = s.timing()
     d = s.diagnostics()
     return dict(solver=s, ms=ms, iters=iters, warm_iters=warm_iters, timing=tm, diag=d,
-                dts=dts, clocks=ck, total_iters=d["total_iterations"] - d0)
+                dts=dts, clocks=ck, total_iters=d["total_iterations"] - d0, warm_launches=warm_launches)
+
+
+def nvtx_mod():
+    try:
+        import torch
+        return torch.cuda.nvtx
+    except Exception:
+        return None
 
 
 def log(msg):
@@ -223,6 +236,11 @@ def reference_sample(q0, p, sor_iters=10):
     r.close()
     return t_h, t_it
 
+
+# DRAM bytes (read + write) per grid cell of one launch, from ncu captures of
+# the 256^3 workload (profiles/sor_split_kernel_fp{32,64}_stellar_explosion_256.txt),
+# keyed by kernel and word size.
+NCU_DRAM_BYTES_PER_CELL = {("sor_split_kernel", 4): 6.47, ("sor_split_kernel", 8): 14.38}
 
 REF_ITERS_FILE = os.path.join(ROOT, "hydrocode_astro1_b200", "data", "fp64_iterations.json")
 
@@ -299,21 +317,24 @@ def main_ours(args):
     s = r["solver"]
     fp64 = variant.startswith("fp64")
 
-    # roofline of the dominant kernel family (SOR sweeps)
+    # roofline of the dominant kernel: one colour sweep of the colour-split SOR
+    # (sor_split_kernel).  Algorithmic bytes: half an iteration's 24 B/cell
+    # (FP64 phi read + write, rho read) or 12 B/cell (FP32 e read + write, r
+    # read) over the interior cells.
     interior = (p["shape"][0] - 2) * (p["shape"][1] - 2) * (p["shape"][2] - 2)
-    if fp64:
-        bytes_per_launch = interior * 24 / 2.0     # one colour sweep: half of 24 B/cell/iteration
-    else:
-        bytes_per_launch = interior * 12 / 2.0     # FP32 correction: e r/w + r read per iteration
+    word = 8 if fp64 else 4
+    bytes_per_launch = interior * 3 * word / 2.0
     sor_launches = max(tm["sor_launches"], 1)
     sor_avg_ms = tm["sor_ms"] / sor_launches
     pk, pk_kind = peaks()
     achieved = bytes_per_launch / (sor_avg_ms / 1e3) / 1e9 if sor_avg_ms > 0 else 0.0
-    dominant = "sor_sweep"
     shares = {k: tm[k] for k in ("hydro_ms", "bc_ms", "sor_ms", "residual_ms", "moments_ms", "unet_ms")}
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": pk, "unit": "GB/s",
-                "frac": achieved / pk, "peak_kind": pk_kind, "traffic": None,
+    traffic = NCU_DRAM_BYTES_PER_CELL.get(("sor_split_kernel", word))
+    roofline = {"bound": "hbm", "kernel": "sor_split_kernel", "achieved": achieved, "peak": pk, "unit": "GB/s",
+                "frac": achieved / pk, "peak_kind": pk_kind,
+                "traffic": traffic * ncell if traffic else None,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
+                "layout_bytes_per_launch": 4 * word * ncell / 2.0,
                 "avg_launch_ms": sor_avg_ms, "launches": tm["sor_launches"]}
     hydro_bytes = interior * (48 if not fp64 else 88)
     hydro_avg = tm["hydro_ms"] / max(tm["hydro_launches"], 1)
@@ -338,6 +359,7 @@ def main_ours(args):
         "roofline": roofline,
         "roofline_hydro": hydro_roof,
         "gpu_launches": tm["launches"],
+        "warmup_gpu_launches": r["warm_launches"],
         "clocks": r["clocks"],
     }
 
