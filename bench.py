@@ -215,6 +215,23 @@ def peaks():
 
 
 # ---------------------------------------------------------------- reference arm
+class stdout_to_stderr:
+    """Send file descriptor 1 to stderr while the reference's C code runs (it
+    prints banners to stdout); the bench's stdout carries one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        return False
+
+
 def reference_sample(q0, p, sor_iters=10):
     """Time the reference's own C code (oracle/_ref) on one bounded sample of a
     step: one hydro step (godunov_step_3d with gravity off) and `sor_iters`
@@ -222,18 +239,19 @@ def reference_sample(q0, p, sor_iters=10):
     re-evaluates the multipole boundary (gravity_solver_3d.c:712).  Returns
     (t_hydro_s, t_iter_s)."""
     from oracle.oracle import RefSim
-    r = RefSim(*p["shape"], lo=p["lo"], hi=p["hi"], G=p["G"], gamma=p["gamma"], cfl=p["cfl"],
-               bc=p["bc"], omega=1.5, max_iter=sor_iters, tol=0.0, grav_bc=1)
-    r.set_state(q0)
-    r.enable_gravity(False)
-    t = time.perf_counter()
-    r.step(1)
-    t_h = time.perf_counter() - t
-    rho = q0[0]
-    t = time.perf_counter()
-    r.gravity_solve(rho, potential_only=True)
-    t_it = (time.perf_counter() - t) / sor_iters
-    r.close()
+    with stdout_to_stderr():
+        r = RefSim(*p["shape"], lo=p["lo"], hi=p["hi"], G=p["G"], gamma=p["gamma"], cfl=p["cfl"],
+                   bc=p["bc"], omega=1.5, max_iter=sor_iters, tol=0.0, grav_bc=1)
+        r.set_state(q0)
+        r.enable_gravity(False)
+        t = time.perf_counter()
+        r.step(1)
+        t_h = time.perf_counter() - t
+        rho = q0[0]
+        t = time.perf_counter()
+        r.gravity_solve(rho, potential_only=True)
+        t_it = (time.perf_counter() - t) / sor_iters
+        r.close()
     return t_h, t_it
 
 

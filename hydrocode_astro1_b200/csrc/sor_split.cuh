@@ -53,7 +53,11 @@ constexpr int SPLIT_BX = 32, SPLIT_BY = 8;
 
 // One thread owns the column (j, m) over NI consecutive planes i0..i0+NI-1:
 // every operand of the NI updates is loaded first (6 NI + 2 independent
-// loads in flight per thread), then the updates run and are stored.
+// loads in flight per thread), then the updates run and are stored.  Offsets
+// are 32-bit (a colour array holds < 2^31 cells).  Loads need no clamping:
+// the z neighbour across a row end is a real cell of the adjacent row (rows
+// j-1 and j+1 exist for 1 <= j <= ny-2) and feeds only boundary cells, and a
+// CTA whose planes reach past nx-2 takes the guarded tail path.
 template <typename T, typename S, int NI>
 __global__ void __launch_bounds__(SPLIT_BX * SPLIT_BY)
 sor_split_kernel(T *__restrict__ own, const T *__restrict__ oth, const S *__restrict__ src, Split sp,
@@ -76,43 +80,56 @@ sor_split_kernel(T *__restrict__ own, const T *__restrict__ oth, const S *__rest
     const int i0 = 1 + blockIdx.z * NI;
     T rmax = (T)0;
     if (j >= 1 && j <= sp.ny - 2 && m < sp.H) {
-        const long long sJ = sp.H, sI = (long long)sp.ny * sp.H;
-        const long long o0 = (long long)i0 * sI + (long long)j * sJ + m;
-        const int ilast = sp.nx - 2;                 // last interior plane
-        // x column: planes i0-1 .. i0+NI, clamped to the grid
-        T x[NI + 2];
-#pragma unroll
-        for (int q = 0; q < NI + 2; q++) {
-            const int i = min(i0 - 1 + q, ilast + 1);
-            x[q] = oth[o0 + (long long)(i - i0) * sI];
-        }
-        T ym[NI], yp[NI], zo[NI], ow[NI];
+        const int sJ = sp.H, sI = sp.ny * sp.H;
+        const int o0 = i0 * sI + j * sJ + m;
+        const int s0 = (i0 + j + colour) & 1;
+        // interior in k for s = 0 (k = 2m) and s = 1 (k = 2m+1)
+        const bool ok0 = m >= 1 && 2 * m <= sp.nz - 2;
+        const bool ok1 = 2 * m + 1 <= sp.nz - 2;
+        const int nq = min(NI, sp.nx - 1 - i0);   // planes i0 .. i0+nq-1 are interior
+        const T *ox = oth + o0;
+        const S *sx = src + o0;
+        T *wx = own + o0;
+        T x[NI + 2], ym[NI], yp[NI], zo[NI], ow[NI];
         S sr[NI];
+        if (nq == NI) {
 #pragma unroll
-        for (int q = 0; q < NI; q++) {
-            const int i = min(i0 + q, ilast);
-            const long long o = o0 + (long long)(i - i0) * sI;
-            const long long row = o - m;             // first element of row (i, j)
-            const int s = (i + j + colour) & 1;
-            ym[q] = oth[o - sJ];
-            yp[q] = oth[o + sJ];
-            // the z neighbour that is not in this column: m-1 (s = 0) or m+1
-            // (s = 1), clamped to the row (only interior cells use it)
-            zo[q] = oth[s ? min(o + 1, row + sp.H - 1) : max(o - 1, row)];
-            ow[q] = own[o];
-            sr[q] = src[o];
+            for (int q = 0; q < NI + 2; q++) x[q] = ox[(q - 1) * sI];
+#pragma unroll
+            for (int q = 0; q < NI; q++) {
+                const int s = s0 ^ (q & 1);
+                ym[q] = ox[q * sI - sJ];
+                yp[q] = ox[q * sI + sJ];
+                zo[q] = ox[q * sI + (s ? 1 : -1)];
+                ow[q] = wx[q * sI];
+                sr[q] = sx[q * sI];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < NI + 2; q++) x[q] = (q <= nq + 1) ? ox[(q - 1) * sI] : (T)0;
+#pragma unroll
+            for (int q = 0; q < NI; q++) {
+                const int s = s0 ^ (q & 1);
+                if (q < nq) {
+                    ym[q] = ox[q * sI - sJ];
+                    yp[q] = ox[q * sI + sJ];
+                    zo[q] = ox[q * sI + (s ? 1 : -1)];
+                    ow[q] = wx[q * sI];
+                    sr[q] = sx[q * sI];
+                } else {
+                    ym[q] = yp[q] = zo[q] = ow[q] = (T)0;
+                    sr[q] = (S)0;
+                }
+            }
         }
 #pragma unroll
         for (int q = 0; q < NI; q++) {
-            const int i = i0 + q;
-            const int s = (i + j + colour) & 1;
-            const int k = 2 * m + s;
-            if (i <= ilast && k >= 1 && k <= sp.nz - 2) {
+            const int s = s0 ^ (q & 1);
+            if (q < nq && (s ? ok1 : ok0)) {
                 const T zm = s ? x[q + 1] : zo[q];
                 const T zp = s ? zo[q] : x[q + 1];
                 T r;
-                own[o0 + (long long)q * sI] =
-                    cf.update(ow[q], x[q], x[q + 2], ym[q], yp[q], zm, zp, (T)sr[q], r);
+                wx[q * sI] = cf.update(ow[q], x[q], x[q + 2], ym[q], yp[q], zm, zp, (T)sr[q], r);
                 rmax = tmax(rmax, r);
             }
         }
@@ -172,7 +189,8 @@ template <typename T, typename S>
 cudaError_t launch_sor_split(T *base, const S *src, const Split &sp, const SorCoef<T> &cf, int colour,
                              double *res, int iter, double thresh, DevScalars *sc, cudaStream_t s)
 {
-    constexpr int NI = sizeof(T) == 8 ? 2 : 4;
+    constexpr int NI = sizeof(T) == 8 ? 4 : 8;   // fastest at 256^3 (FP64 55.6, FP32 31.2 us per sweep)
+    if (sp.cs + 2LL * sp.ny * sp.H >= (1LL << 31)) return cudaErrorInvalidValue;   // 32-bit offsets
     dim3 grid((sp.H + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + NI - 1) / NI);
     T *own = base + (size_t)colour * sp.cs;
     const T *oth = base + (size_t)(colour ^ 1) * sp.cs;
