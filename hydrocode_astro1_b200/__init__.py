@@ -96,6 +96,10 @@ CAPI = {
     "hc_timer_stop": (C.c_int, [C.c_void_p, _dp]),
     "hc_unet_param_count": (C.c_int, []),
     "hc_unet_load": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint16), C.c_int]),
+    "hc_unet_conv_test": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
+                                    C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(C.c_float)]),
+    "hc_unet_wgrad_test": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
+                                     C.c_int, C.POINTER(C.c_float)]),
     "hc_sor_solve_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
                                         C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                         C.c_double, C.c_void_p, C.POINTER(C.c_int), _dp]),

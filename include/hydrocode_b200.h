@@ -179,6 +179,19 @@ int hc_timer_stop(hc_ctx *ctx, double *ms);
 int hc_unet_param_count(void);
 int hc_unet_load(hc_ctx *ctx, const uint16_t *w_bf16, int nparam);
 
+/* Diagnostics of the tensor-core convolution kernels (no reference
+ * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16
+ * channels (channels last), weights w[co][tap][ci] (16*27*16 BF16, tap =
+ * (di+1)*9 + (dj+1)*3 + (dk+1)), bias[16] FP32.
+ * hc_unet_conv_test: 3x3x3 zero-padded convolution; out_mode 0: +bias,
+ * LeakyReLU(0.1) if act, BF16-rounded, 16 channels; 1: BF16, no bias; 2: FP32
+ * channel 0 + bias[0]; 3: FP32 16 channels + bias; `out` receives FP32.
+ * hc_unet_wgrad_test: dw[co][tap][ci] = sum_v dy[v][co] x[v+tap][ci] (FP32),
+ * reduced over at most max_parts partial sums. */
+int hc_unet_conv_test(int nx, int ny, int nz, const uint16_t *x, const uint16_t *w, const float *bias,
+                      int out_mode, int act, float *out);
+int hc_unet_wgrad_test(int nx, int ny, int nz, const uint16_t *x, const uint16_t *dy, int max_parts, float *dw);
+
 /* Red-black SOR to tolerance on caller-owned DEVICE arrays, allocating
  * nothing.  No counterpart in the reference: it exists for callers that own
  * all device memory themselves (a fixed arena reserved at start-up, a pool
