@@ -25,6 +25,7 @@ BC_PERIODIC, BC_REFLECTIVE, BC_OUTFLOW = 0, 1, 2
 GRAV_BC_PERIODIC, GRAV_BC_ISOLATED, GRAV_BC_DIRICHLET = 0, 1, 2
 FP64, FP32 = 0, 1
 MOMENTS_SEQUENTIAL, MOMENTS_TREE = 0, 1
+HC_WARM_PREVIOUS, HC_WARM_UNET = 0, 1
 WARM_PREVIOUS, WARM_UNET = 0, 1
 
 HC_OK, HC_NOT_CONVERGED = 0, -1
@@ -53,6 +54,7 @@ class Diag(C.Structure):
         ("last_status", C.c_int), ("warm_start_used", C.c_int),
         ("outer_cycles", C.c_int), ("dt", C.c_double), ("steps", C.c_longlong),
         ("total_iterations", C.c_longlong), ("overshoot", C.c_int),
+        ("unet_accepted", C.c_longlong), ("unet_fallbacks", C.c_longlong),
     ]
 
 
@@ -95,7 +97,17 @@ CAPI = {
     "hc_timer_start": (C.c_int, [C.c_void_p]),
     "hc_timer_stop": (C.c_int, [C.c_void_p, _dp]),
     "hc_unet_param_count": (C.c_int, []),
-    "hc_unet_load": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint16), C.c_int]),
+    "hc_unet_init": (C.c_int, [C.c_void_p, C.c_uint]),
+    "hc_unet_load": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_double]),
+    "hc_unet_save": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_double)]),
+    "hc_unet_load_file": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "hc_unet_save_file": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "hc_unet_collect": (C.c_int, [C.c_void_p, C.c_int]),
+    "hc_unet_samples": (C.c_int, [C.c_void_p]),
+    "hc_unet_train": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint, C.POINTER(C.c_double)]),
+    "hc_unet_loss_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float)]),
     "hc_unet_conv_test": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
                                     C.POINTER(C.c_float), C.c_int, C.c_int, C.POINTER(C.c_float)]),
     "hc_unet_wgrad_test": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
@@ -300,6 +312,52 @@ class HydroSolver3D:
         v = C.c_double(0.0)
         _check(self.L.hc_timer_stop(self.h, C.byref(v)), "hc_timer_stop")
         return v.value
+
+    # learned warm start --------------------------------------------------------
+    def unet_init(self, seed=0):
+        _check(self.L.hc_unet_init(self.h, seed), "hc_unet_init")
+
+    def unet_load(self, params, kscale):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        _check(self.L.hc_unet_load(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size, float(kscale)),
+               "hc_unet_load")
+
+    def unet_params(self):
+        n = self.L.hc_unet_param_count()
+        p = np.zeros(n, np.float32)
+        k = C.c_double(0.0)
+        _check(self.L.hc_unet_save(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), n, C.byref(k)), "hc_unet_save")
+        return p, k.value
+
+    def unet_load_file(self, path):
+        _check(self.L.hc_unet_load_file(self.h, str(path).encode()), "hc_unet_load_file")
+
+    def unet_save_file(self, path):
+        _check(self.L.hc_unet_save_file(self.h, str(path).encode()), "hc_unet_save_file")
+
+    def unet_collect(self, capacity):
+        _check(self.L.hc_unet_collect(self.h, int(capacity)), "hc_unet_collect")
+
+    def unet_samples(self):
+        return self.L.hc_unet_samples(self.h)
+
+    def unet_train(self, steps, lr=1e-3, seed=0):
+        loss = C.c_double(0.0)
+        _check(self.L.hc_unet_train(self.h, int(steps), float(lr), int(seed), C.byref(loss)), "hc_unet_train")
+        return loss.value
+
+    def unet_loss_grad(self, x, t):
+        """One forward/backward pass at the network's level-0 dims (x.shape)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        n = self.L.hc_unet_param_count()
+        g = np.zeros(n, np.float32)
+        out = np.zeros(x.shape, np.float32)
+        loss = C.c_double(0.0)
+        fp = C.POINTER(C.c_float)
+        _check(self.L.hc_unet_loss_grad(self.h, *x.shape, x.ctypes.data_as(fp), t.ctypes.data_as(fp), C.byref(loss),
+                                        g.ctypes.data_as(fp), out.ctypes.data_as(fp)), "hc_unet_loss_grad")
+        return loss.value, g, out
 
 
 def pin(array):

@@ -94,7 +94,7 @@ struct hc_ctx {
     std::vector<EvPair> pend;
     std::vector<cudaEvent_t> evpool;
     // learned warm start
-    void *unet;
+    UNetState *unet;
     // user timer
     cudaEvent_t t0, t1;
     int timer_on;
@@ -202,8 +202,7 @@ static void free_ctx(hc_ctx *c)
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
     if (c->s) cudaStreamDestroy(c->s);
-    extern void hc_unet_free(void *);
-    if (c->unet) hc_unet_free(c->unet);
+    unet_destroy(c->unet);
     delete c;
 }
 
@@ -637,7 +636,8 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
     if (rc) return rc;
     int total = 0, cycles = 0, status = -1;
     double dmax = 0.0;
-    while (true) {
+    // FP64 residual delta of phi into r32 (e32 zeroed); returns max|delta|
+    auto residual = [&](double *out) -> int {
         {
             FamTimer t(c, FAM_RES);
             CK(cudaMemsetAsync(&c->sc->resnorm, 0, sizeof(double), c->s));
@@ -645,11 +645,52 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
             c->launches++;
         }
         CK(cudaMemcpyAsync(&c->hsc->resnorm, &c->sc->resnorm, sizeof(double), cudaMemcpyDeviceToHost, c->s));
-        rc = sync_ctx(c);
-        if (rc) return rc;
+        int r = sync_ctx(c);
+        if (r) return r;
+        *out = c->hsc->resnorm;
+        return HC_OK;
+    };
+    c->diag.warm_start_used = 0;
+    bool recorded = false;
+    while (true) {
         const double prev_dmax = cycles ? dmax : 1e300;
-        dmax = c->hsc->resnorm;
+        rc = residual(&dmax);
+        if (rc) return rc;
         cycles++;
+        // Learned warm start (first cycle, colour-split layout): the network
+        // predicts the correction from this residual; phi + e0 is kept only
+        // if its FP64 residual is smaller, else phi is restored.  With sample
+        // collection on, the residual and phi are recorded for training.
+        if (cycles == 1 && split && c->unet && std::isfinite(dmax)) {
+            const bool predict = c->cfg.warm_start == HC_WARM_UNET && unet_has_weights(c->unet);
+            if (predict || unet_collecting(c->unet)) {
+                {
+                    FamTimer t(c, FAM_UNET);
+                    rc = unet_begin_solve(c->unet, a, c->r32, predict ? c->e32b : nullptr, c->s);
+                    c->launches += predict ? 40 : 3;
+                }
+                if (rc) return set_err(rc, "learned warm start: grid dimensions must be multiples of 16");
+                recorded = unet_collecting(c->unet);
+            }
+            if (predict) {
+                CK(mixed_update(a, c->e32b, split, 1.0f, c->s));
+                double d1 = 0.0;
+                rc = residual(&d1);
+                if (rc) return rc;
+                if (c->debug) fprintf(stderr, "[hc] learned start: max|delta| %.3e -> %.3e\n", dmax, d1);
+                if (std::isfinite(d1) && d1 < dmax) {
+                    dmax = d1;
+                    c->diag.warm_start_used = 1;
+                    c->diag.unet_accepted++;
+                } else {
+                    CK(mixed_update(a, c->e32b, split, -1.0f, c->s));
+                    rc = residual(&dmax);
+                    if (rc) return rc;
+                    c->diag.unet_fallbacks++;
+                }
+                c->launches += 2;
+            }
+        }
         if (c->debug) fprintf(stderr, "[hc] mixed cycle %d: max|delta| %.3e after %d sweeps\n", cycles, dmax, total);
         if (!std::isfinite(dmax)) return set_err(HC_ERR_NUMERIC, "non-finite Poisson residual");
         if (dmax < a.tol) { status = 0; break; }
@@ -734,7 +775,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         {
             FamTimer t(c, FAM_RES);
             CK(cudaMemsetAsync(&c->sc->resid_bits, 0, sizeof(unsigned long long), c->s));
-            CK(mixed_update(a, efinal, split, c->s));
+            CK(mixed_update(a, efinal, split, 1.0f, c->s));
             c->launches++;
         }
         // Converged by the reference's criterion when the last sweep's update
@@ -766,6 +807,10 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
     c->diag.last_residual = dmax;
     c->diag.outer_cycles = cycles;
     c->diag.total_iterations += total;
+    if (recorded) {
+        rc = unet_end_solve(c->unet, a, status == 0, c->s);
+        if (rc) return set_err(rc, "learned warm start: recording a training sample failed");
+    }
     return status;
 }
 
@@ -1154,4 +1199,106 @@ extern "C" int hc_host_unregister(void *ptr)
 int hc_internal_set_error(int code, const char *msg)
 {
     return set_err(code, "%s", msg);
+}
+
+// ---------------------------------------------------------------- learned warm start
+static int ensure_unet(hc_ctx *c)
+{
+    if (c->unet) return HC_OK;
+    CK(cudaSetDevice(c->dev));
+    c->unet = unet_create(c->dev);
+    return c->unet ? HC_OK : set_err(HC_ERR_NOMEM, "U-Net parameter buffers");
+}
+
+extern "C" int hc_unet_param_count(void) { return unet_param_count(); }
+
+extern "C" int hc_unet_init(hc_ctx *c, unsigned seed)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    int rc = ensure_unet(c);
+    return rc ? rc : unet_init(c->unet, seed, c->s);
+}
+
+extern "C" int hc_unet_load(hc_ctx *c, const float *params, int nparam, double kscale)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    int rc = ensure_unet(c);
+    if (rc) return rc;
+    rc = unet_set_params(c->unet, params, nparam, (float)kscale, c->s);
+    return rc ? set_err(rc, "hc_unet_load: expected %d parameters and kscale > 0", unet_param_count()) : HC_OK;
+}
+
+extern "C" int hc_unet_save(hc_ctx *c, float *params, int nparam, double *kscale)
+{
+    if (!c || !c->unet || !unet_has_weights(c->unet)) return set_err(HC_ERR_STATE, "no U-Net weights");
+    if (kscale) *kscale = unet_kscale(c->unet);
+    return unet_get_params(c->unet, params, nparam, c->s);
+}
+
+// file: "HCUNET01", int32 parameter count, float32 kscale, float32 parameters
+extern "C" int hc_unet_save_file(hc_ctx *c, const char *path)
+{
+    const int n = unet_param_count();
+    std::vector<float> p(n);
+    double k = 0.0;
+    int rc = hc_unet_save(c, p.data(), n, &k);
+    if (rc) return rc;
+    FILE *f = fopen(path, "wb");
+    if (!f) return set_err(HC_ERR_ARG, "cannot write %s", path);
+    const float kf = (float)k;
+    bool ok = fwrite("HCUNET01", 1, 8, f) == 8 && fwrite(&n, 4, 1, f) == 1 && fwrite(&kf, 4, 1, f) == 1 &&
+              fwrite(p.data(), 4, n, f) == (size_t)n;
+    ok = (fclose(f) == 0) && ok;
+    return ok ? HC_OK : set_err(HC_ERR_ARG, "short write to %s", path);
+}
+
+extern "C" int hc_unet_load_file(hc_ctx *c, const char *path)
+{
+    FILE *f = fopen(path, "rb");
+    if (!f) return set_err(HC_ERR_ARG, "cannot read %s", path);
+    char magic[8];
+    int n = 0;
+    float k = 0.f;
+    bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "HCUNET01", 8) == 0 && fread(&n, 4, 1, f) == 1 &&
+              fread(&k, 4, 1, f) == 1 && n == unet_param_count();
+    std::vector<float> p(ok ? n : 0);
+    ok = ok && fread(p.data(), 4, n, f) == (size_t)n;
+    fclose(f);
+    if (!ok) return set_err(HC_ERR_ARG, "%s is not a U-Net weight file of %d parameters", path, unet_param_count());
+    return hc_unet_load(c, p.data(), n, k);
+}
+
+extern "C" int hc_unet_collect(hc_ctx *c, int capacity)
+{
+    if (!c || capacity < 0) return set_err(HC_ERR_ARG, "bad argument");
+    int rc = ensure_unet(c);
+    if (rc) return rc;
+    rc = unet_collect(c->unet, capacity);
+    return rc ? set_err(rc, "sample buffers") : HC_OK;
+}
+
+extern "C" int hc_unet_samples(hc_ctx *c) { return (c && c->unet) ? unet_samples(c->unet) : 0; }
+
+extern "C" int hc_unet_train(hc_ctx *c, int steps, double lr, unsigned seed, double *mean_loss)
+{
+    if (!c || !c->unet) return set_err(HC_ERR_STATE, "no U-Net");
+    CK(cudaSetDevice(c->dev));
+    int rc;
+    {
+        FamTimer t(c, FAM_UNET);
+        rc = unet_train(c->unet, steps, lr, seed, mean_loss, c->s);
+    }
+    if (rc == HC_ERR_STATE) return set_err(rc, "no training samples (hc_unet_collect, then solve)");
+    if (rc) return set_err(rc, "U-Net training failed");
+    return sync_ctx(c);
+}
+
+extern "C" int hc_unet_loss_grad(hc_ctx *c, int nx, int ny, int nz, const float *x, const float *t, double *loss,
+                                 float *grad, float *out)
+{
+    if (!c || !c->unet || !x || !t || nx < 2 || ny < 2 || nz < 2 || nx % 8 || ny % 8 || nz % 8)
+        return set_err(HC_ERR_ARG, "bad argument (level-0 dimensions must be multiples of 8)");
+    CK(cudaSetDevice(c->dev));
+    const int rc = unet_loss_grad(c->unet, nx, ny, nz, x, t, loss, grad, out, c->s);
+    return rc ? set_err(rc, "U-Net loss/gradient failed") : HC_OK;
 }

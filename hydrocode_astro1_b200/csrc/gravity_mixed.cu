@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(256) mixed_residual_kernel(GravArgs a, float *
 }
 
 // phi += e; max|e| into sc->resid_bits (the FP32 resolution check)
-__global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const float *e32, Split sp)
+__global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const float *e32, Split sp, float sign)
 {
     const long long sI = (long long)a.g.ny * a.g.nz, sJ = a.g.nz;
     float m = 0.f;
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const flo
          c += (long long)gridDim.x * blockDim.x) {
         long long o = c;
         if (sp.cs) o = sp.at((int)(c / sI), (int)((c / sJ) % a.g.ny), (int)(c % sJ));
-        const float e = e32[o];
+        const float e = sign * e32[o];
         a.phi[c] += (double)e;
         m = tmax(m, fabsf(e));
     }
@@ -365,9 +365,9 @@ cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, bool split
     return cudaGetLastError();
 }
 
-cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, cudaStream_t s)
+cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, float sign, cudaStream_t s)
 {
-    mixed_update_kernel<<<148 * 8, 256, 0, s>>>(a, e32, split_or_natural(a, split));
+    mixed_update_kernel<<<148 * 8, 256, 0, s>>>(a, e32, split_or_natural(a, split), sign);
     return cudaGetLastError();
 }
 

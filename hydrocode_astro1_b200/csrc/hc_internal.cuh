@@ -157,7 +157,7 @@ int lmax_ncoef(int lmax);
 namespace hc {
 // split: r32 / e32 in the colour-split layout of sor_split.cuh
 cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, bool split, cudaStream_t s);
-cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, cudaStream_t s);
+cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, float sign, cudaStream_t s);
 cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, int colour, int iter,
                               double thresh, cudaStream_t s);
 cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int color, int iter,
@@ -177,4 +177,26 @@ cudaError_t grav_unsplit(const GravArgs &a, const double *phs, cudaStream_t s);
 cudaError_t grav_sor_split(const GravArgs &a, double *phs, const double *rhs, int colour, int iter, cudaStream_t s);
 cudaError_t mixed_sor32_pass(const GravArgs &a, const float *in, float *out, const float *r32, int iter0,
                              int depth, double thresh, cudaStream_t s);
+}  // namespace hc
+
+// Learned warm start (unet.cu): a 3D U-Net on the half-resolution grid that
+// predicts the correction of a mixed-precision solve from its first residual.
+namespace hc {
+struct UNetState;
+int unet_param_count();
+UNetState *unet_create(int dev);
+void unet_destroy(UNetState *u);
+bool unet_has_weights(const UNetState *u);
+float unet_kscale(const UNetState *u);
+int unet_set_params(UNetState *u, const float *compact, int n, float kscale, cudaStream_t s);
+int unet_get_params(UNetState *u, float *compact, int n, cudaStream_t s);
+int unet_init(UNetState *u, unsigned seed, cudaStream_t s);
+int unet_collect(UNetState *u, int capacity);
+int unet_samples(const UNetState *u);
+bool unet_collecting(const UNetState *u);
+int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e_out, cudaStream_t s);
+int unet_end_solve(UNetState *u, const GravArgs &a, bool converged, cudaStream_t s);
+int unet_train(UNetState *u, int steps, double lr, unsigned seed, double *mean_loss, cudaStream_t s);
+int unet_loss_grad(UNetState *u, int n0x, int n0y, int n0z, const float *x, const float *t, double *loss, float *grad,
+                   float *out, cudaStream_t s);
 }  // namespace hc

@@ -3,10 +3,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <random>
 #include <vector>
 
 #include "../../include/hydrocode_b200.h"
+#include "hc_internal.cuh"
 #include "unet_conv.cuh"
 
 namespace hc {
@@ -43,6 +46,499 @@ cudaError_t wgrad(const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *dw, fl
 }
 
 }  // namespace unet
+}  // namespace hc
+
+// ---------------------------------------------------------------------------
+// The network: a 3D U-Net on the half-resolution grid of the solve.
+//   x0 (channel 0 = 2x-pooled FP64 residual / its RMS)
+//   e0 = f(conv0 x0)                 level 0 (grid / 2)
+//   e1 = f(conv1 pool e0)            level 1
+//   e2 = f(conv2 pool e1)            level 2
+//   e3 = f(conv3 pool e2), b = f(conv4 e3)      level 3
+//   d2 = f(conv5 (up b + e2)), d1 = f(conv6 (up d2 + e1)), d0 = f(conv7 (up d1 + e0))
+//   out = conv8 d0 (channel 0)
+// f = LeakyReLU(0.1); pool = 2x average; up = 2x nearest.  16 channels at
+// every level; 49,377 trainable parameters.  The correction of the solve is
+//   e = trilinear_up(out) * RMS(pooled residual) * kscale.
+// ---------------------------------------------------------------------------
+#include "unet_ops.cuh"
+
+namespace hc {
+
+namespace unet {
+constexpr int NCONV = 9;
+constexpr int PFULL = WELEM + CH;                 // weights + bias of one conv, full layout
+constexpr int NFULL = NCONV * PFULL;
+constexpr int NPARAM = (CH * NTAP + CH) + 7 * (WELEM + CH) + (NTAP * CH + 1);   // 49377
+constexpr int MAX_PARTS = 148;
+}  // namespace unet
+
+using namespace unet;
+
+struct UNetState {
+    int dev = 0;
+    float kscale = 30.f;
+    bool have_weights = false;
+    int adam_t = 0;
+    // parameters (full layout, FP32) and Adam moments, gradients
+    float *pm = nullptr, *pg = nullptr, *am = nullptr, *av = nullptr;
+    __nv_bfloat16 *wf = nullptr, *wt = nullptr;    // NCONV x WELEM each
+    // buffers for one grid size
+    int gx = 0, gy = 0, gz = 0;
+    Dims L[4];
+    __nv_bfloat16 *x0, *e0, *s0, *d0, *g0a, *g0b;
+    __nv_bfloat16 *p1, *e1, *s1, *d1, *g1a, *g1b, *g1c;
+    __nv_bfloat16 *p2, *e2, *s2, *d2, *g2a, *g2b, *g2c;
+    __nv_bfloat16 *p3, *e3, *bb, *g3a, *g3b;
+    float *out0 = nullptr, *pooled = nullptr, *xnorm = nullptr, *partial = nullptr, *bpart = nullptr;
+    double *scal = nullptr;       // [0] sumsq of the input, [1] sum t^2, [2] loss
+    int *err = nullptr;
+    void *act_mem = nullptr;
+    // training samples: normalised inputs and targets at level 0
+    int cap = 0, count = 0, next = 0, slot = -1;
+    float *sx = nullptr, *st = nullptr;
+    std::vector<double> st2;
+    double *phi0 = nullptr;
+    long long phi0_n = 0;
+    std::vector<void *> fixed;
+};
+
+namespace {
+int dalloc(void **p, size_t bytes)
+{
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        *p = nullptr;
+        return HC_ERR_NOMEM;
+    }
+    return HC_OK;
+}
+inline unsigned nblk(long long n, int nt = 256)
+{
+    long long b = (n + nt - 1) / nt;
+    return (unsigned)std::max<long long>(1, std::min<long long>(b, 148LL * 16));
+}
+__nv_bfloat16 *wf_of(UNetState *u, int l) { return u->wf + (size_t)l * WELEM; }
+__nv_bfloat16 *wt_of(UNetState *u, int l) { return u->wt + (size_t)l * WELEM; }
+float *bias_of(UNetState *u, int l) { return u->pm + (size_t)l * PFULL + WELEM; }
+
+// compact <-> full parameter layouts (host)
+void compact_to_full(const float *c, std::vector<float> &f)
+{
+    f.assign(NFULL, 0.f);
+    size_t q = 0;
+    for (int l = 0; l < NCONV; l++) {
+        float *w = f.data() + (size_t)l * PFULL, *b = w + WELEM;
+        if (l == 0) {
+            for (int co = 0; co < CH; co++)
+                for (int tap = 0; tap < NTAP; tap++) w[(co * NTAP + tap) * CH] = c[q++];
+            for (int co = 0; co < CH; co++) b[co] = c[q++];
+        } else if (l == NCONV - 1) {
+            for (int tap = 0; tap < NTAP; tap++)
+                for (int ci = 0; ci < CH; ci++) w[tap * CH + ci] = c[q++];
+            b[0] = c[q++];
+        } else {
+            for (int e = 0; e < WELEM; e++) w[e] = c[q++];
+            for (int co = 0; co < CH; co++) b[co] = c[q++];
+        }
+    }
+}
+void full_to_compact(const std::vector<float> &f, float *c)
+{
+    size_t q = 0;
+    for (int l = 0; l < NCONV; l++) {
+        const float *w = f.data() + (size_t)l * PFULL, *b = w + WELEM;
+        if (l == 0) {
+            for (int co = 0; co < CH; co++)
+                for (int tap = 0; tap < NTAP; tap++) c[q++] = w[(co * NTAP + tap) * CH];
+            for (int co = 0; co < CH; co++) c[q++] = b[co];
+        } else if (l == NCONV - 1) {
+            for (int tap = 0; tap < NTAP; tap++)
+                for (int ci = 0; ci < CH; ci++) c[q++] = w[tap * CH + ci];
+            c[q++] = b[0];
+        } else {
+            for (int e = 0; e < WELEM; e++) c[q++] = w[e];
+            for (int co = 0; co < CH; co++) c[q++] = b[co];
+        }
+    }
+}
+
+cudaError_t pack_all(UNetState *u, cudaStream_t s)
+{
+    for (int l = 0; l < NCONV; l++)
+        pack_weights_kernel<<<(WELEM + 255) / 256, 256, 0, s>>>(u->pm + (size_t)l * PFULL, wf_of(u, l), wt_of(u, l));
+    return cudaGetLastError();
+}
+
+void free_grid(UNetState *u)
+{
+    cudaFree(u->act_mem);
+    u->act_mem = nullptr;
+    u->gx = u->gy = u->gz = 0;
+}
+
+// Buffers for a solve grid of gx x gy x gz cells (each a multiple of 16).
+int ensure_grid(UNetState *u, int gx, int gy, int gz)
+{
+    if (gx % 16 || gy % 16 || gz % 16) return HC_ERR_ARG;
+    if (u->gx == gx && u->gy == gy && u->gz == gz) return HC_OK;
+    free_grid(u);
+    for (int l = 0; l < 4; l++) {
+        const int f = 2 << l;
+        u->L[l] = Dims{ gx / f, gy / f, gz / f, (long long)(gx / f) * (gy / f) * (gz / f) };
+    }
+    const size_t v0 = (size_t)u->L[0].n * CH, v1 = (size_t)u->L[1].n * CH, v2 = (size_t)u->L[2].n * CH,
+                 v3 = (size_t)u->L[3].n * CH;
+    const size_t nbf = 6 * v0 + 7 * v1 + 7 * v2 + 5 * v3;
+    const size_t nf = 3 * (size_t)u->L[0].n + (size_t)MAX_PARTS * WG_MT * TM * CH + 148 * 16 * CH;
+    const size_t bytes = nbf * 2 + nf * 4 + 4 * sizeof(double) + 256 * 4;
+    if (dalloc(&u->act_mem, bytes)) return HC_ERR_NOMEM;
+    char *p = (char *)u->act_mem;
+    auto take_bf = [&](size_t n) { __nv_bfloat16 *r = (__nv_bfloat16 *)p; p += n * 2; return r; };
+    u->x0 = take_bf(v0); u->e0 = take_bf(v0); u->s0 = take_bf(v0); u->d0 = take_bf(v0); u->g0a = take_bf(v0); u->g0b = take_bf(v0);
+    u->p1 = take_bf(v1); u->e1 = take_bf(v1); u->s1 = take_bf(v1); u->d1 = take_bf(v1); u->g1a = take_bf(v1); u->g1b = take_bf(v1); u->g1c = take_bf(v1);
+    u->p2 = take_bf(v2); u->e2 = take_bf(v2); u->s2 = take_bf(v2); u->d2 = take_bf(v2); u->g2a = take_bf(v2); u->g2b = take_bf(v2); u->g2c = take_bf(v2);
+    u->p3 = take_bf(v3); u->e3 = take_bf(v3); u->bb = take_bf(v3); u->g3a = take_bf(v3); u->g3b = take_bf(v3);
+    auto take_f = [&](size_t n) { float *r = (float *)p; p += n * 4; return r; };
+    u->out0 = take_f(u->L[0].n); u->pooled = take_f(u->L[0].n); u->xnorm = take_f(u->L[0].n);
+    u->partial = take_f((size_t)MAX_PARTS * WG_MT * TM * CH);
+    u->bpart = take_f(148 * 16 * CH);
+    p = (char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    u->scal = (double *)p; p += 4 * sizeof(double);
+    u->err = (int *)p;
+    u->gx = gx; u->gy = gy; u->gz = gz;
+    // samples of another grid size are dropped
+    cudaFree(u->sx); cudaFree(u->st);
+    u->sx = u->st = nullptr;
+    u->count = u->next = 0;
+    u->slot = -1;
+    u->st2.clear();
+    if (u->cap > 0) {
+        if (dalloc((void **)&u->sx, (size_t)u->cap * u->L[0].n * 4) ||
+            dalloc((void **)&u->st, (size_t)u->cap * u->L[0].n * 4))
+            return HC_ERR_NOMEM;
+        u->st2.assign(u->cap, 0.0);
+    }
+    cudaMemset(u->err, 0, 4);
+    return HC_OK;
+}
+
+cudaError_t conv_fwd(UNetState *u, int l, const __nv_bfloat16 *x, void *out, int lev, int mode, cudaStream_t s)
+{
+    return conv3(x, wf_of(u, l), bias_of(u, l), out, u->L[lev], mode, mode == 0 ? 1 : 0, u->err, s);
+}
+cudaError_t conv_dgrad(UNetState *u, int l, const __nv_bfloat16 *dy, __nv_bfloat16 *dx, int lev, cudaStream_t s)
+{
+    return conv3(dy, wt_of(u, l), bias_of(u, l), dx, u->L[lev], 1, 0, u->err, s);
+}
+cudaError_t conv_wgrad(UNetState *u, int l, const __nv_bfloat16 *x, const __nv_bfloat16 *dz, int lev, cudaStream_t s)
+{
+    float *g = u->pg + (size_t)l * PFULL;
+    cudaError_t e = wgrad(x, dz, g, u->partial, MAX_PARTS, u->L[lev], u->err, s);
+    if (e != cudaSuccess) return e;
+    const unsigned nb = std::min<unsigned>(148, nblk(u->L[lev].n * 2, BG_NT));
+    bias_grad_kernel<<<nb, BG_NT, 0, s>>>(dz, u->L[lev].n, u->bpart);
+    sum_partials_kernel<<<1, 32, 0, s>>>(u->bpart, nb, g + WELEM, CH);
+    return cudaGetLastError();
+}
+
+cudaError_t forward(UNetState *u, cudaStream_t s)
+{
+    const Dims *L = u->L;
+    cudaError_t e;
+    if ((e = conv_fwd(u, 0, u->x0, u->e0, 0, 0, s))) return e;
+    pool2_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->e0, u->p1, L[1]);
+    if ((e = conv_fwd(u, 1, u->p1, u->e1, 1, 0, s))) return e;
+    pool2_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->e1, u->p2, L[2]);
+    if ((e = conv_fwd(u, 2, u->p2, u->e2, 2, 0, s))) return e;
+    pool2_kernel<<<nblk(L[3].n * 2), 256, 0, s>>>(u->e2, u->p3, L[3]);
+    if ((e = conv_fwd(u, 3, u->p3, u->e3, 3, 0, s))) return e;
+    if ((e = conv_fwd(u, 4, u->e3, u->bb, 3, 0, s))) return e;
+    up_add_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->bb, u->e2, u->s2, L[2]);
+    if ((e = conv_fwd(u, 5, u->s2, u->d2, 2, 0, s))) return e;
+    up_add_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->d2, u->e1, u->s1, L[1]);
+    if ((e = conv_fwd(u, 6, u->s1, u->d1, 1, 0, s))) return e;
+    up_add_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->d1, u->e0, u->s0, L[0]);
+    if ((e = conv_fwd(u, 7, u->s0, u->d0, 0, 0, s))) return e;
+    return conv_fwd(u, 8, u->d0, u->out0, 0, 2, s);
+}
+
+// gradients of the loss whose output gradient is in g0a (channel 0)
+cudaError_t backward(UNetState *u, cudaStream_t s)
+{
+    const Dims *L = u->L;
+    cudaError_t e;
+    // conv8 (no activation)
+    if ((e = conv_wgrad(u, 8, u->d0, u->g0a, 0, s))) return e;
+    if ((e = conv_dgrad(u, 8, u->g0a, u->g0b, 0, s))) return e;
+    act_back_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->g0b, u->d0, u->g0a, L[0].n);   // dz7
+    if ((e = conv_wgrad(u, 7, u->s0, u->g0a, 0, s))) return e;
+    if ((e = conv_dgrad(u, 7, u->g0a, u->g0b, 0, s))) return e;                         // ds0 (skip to e0)
+    downsum_act_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->g0b, u->d1, u->g1a, L[1]);   // dz6
+    if ((e = conv_wgrad(u, 6, u->s1, u->g1a, 1, s))) return e;
+    if ((e = conv_dgrad(u, 6, u->g1a, u->g1b, 1, s))) return e;                         // ds1 (skip to e1)
+    downsum_act_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->g1b, u->d2, u->g2a, L[2]);   // dz5
+    if ((e = conv_wgrad(u, 5, u->s2, u->g2a, 2, s))) return e;
+    if ((e = conv_dgrad(u, 5, u->g2a, u->g2b, 2, s))) return e;                         // ds2 (skip to e2)
+    downsum_act_kernel<<<nblk(L[3].n * 2), 256, 0, s>>>(u->g2b, u->bb, u->g3a, L[3]);   // dz4
+    if ((e = conv_wgrad(u, 4, u->e3, u->g3a, 3, s))) return e;
+    if ((e = conv_dgrad(u, 4, u->g3a, u->g3b, 3, s))) return e;                         // de3
+    act_back_kernel<<<nblk(L[3].n * 2), 256, 0, s>>>(u->g3b, u->e3, u->g3a, L[3].n);    // dz3
+    if ((e = conv_wgrad(u, 3, u->p3, u->g3a, 3, s))) return e;
+    if ((e = conv_dgrad(u, 3, u->g3a, u->g3b, 3, s))) return e;                         // dp3
+    poolback_add_act_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->g2b, u->g3b, u->e2, u->g2a, L[2]);   // dz2
+    if ((e = conv_wgrad(u, 2, u->p2, u->g2a, 2, s))) return e;
+    if ((e = conv_dgrad(u, 2, u->g2a, u->g2c, 2, s))) return e;                         // dp2
+    poolback_add_act_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->g1b, u->g2c, u->e1, u->g1a, L[1]);   // dz1
+    if ((e = conv_wgrad(u, 1, u->p1, u->g1a, 1, s))) return e;
+    if ((e = conv_dgrad(u, 1, u->g1a, u->g1c, 1, s))) return e;                         // dp1
+    poolback_add_act_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->g0b, u->g1c, u->e0, u->g0a, L[0]);   // dz0
+    return conv_wgrad(u, 0, u->x0, u->g0a, 0, s);
+}
+
+// loss (relative squared error) of the current output against target t,
+// with its gradient into g0a; adds loss into scal[2]
+cudaError_t loss_grad(UNetState *u, const float *t, double sumt2, cudaStream_t s)
+{
+    loss_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->out0, t, u->L[0].n, sumt2, u->g0a, u->scal + 2);
+    return cudaGetLastError();
+}
+
+cudaError_t adam_step(UNetState *u, float lr, cudaStream_t s)
+{
+    u->adam_t++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)u->adam_t), c2 = 1.f - powf(b2, (float)u->adam_t);
+    adam_kernel<<<(NFULL + 255) / 256, 256, 0, s>>>(u->pm, u->pg, u->am, u->av, NFULL, lr, b1, b2, 1e-8f, c1, c2);
+    return pack_all(u, s);
+}
+
+int read_err(UNetState *u, cudaStream_t s)
+{
+    int e = 0;
+    if (cudaMemcpyAsync(&e, u->err, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HC_ERR_CUDA;
+    if (e) {
+        cudaMemsetAsync(u->err, 0, 4, s);
+        return HC_ERR_TIMEOUT;
+    }
+    return HC_OK;
+}
+}  // namespace
+
+int unet_param_count() { return NPARAM; }
+
+UNetState *unet_create(int dev)
+{
+    UNetState *u = new UNetState();
+    u->dev = dev;
+    void *m = nullptr;
+    const size_t bytes = (size_t)4 * NFULL * 4 + (size_t)2 * NCONV * WELEM * 2;
+    if (dalloc(&m, bytes)) {
+        delete u;
+        return nullptr;
+    }
+    u->fixed.push_back(m);
+    u->pm = (float *)m;
+    u->pg = u->pm + NFULL;
+    u->am = u->pg + NFULL;
+    u->av = u->am + NFULL;
+    u->wf = (__nv_bfloat16 *)(u->av + NFULL);
+    u->wt = u->wf + (size_t)NCONV * WELEM;
+    cudaMemset(m, 0, bytes);
+    return u;
+}
+
+void unet_destroy(UNetState *u)
+{
+    if (!u) return;
+    free_grid(u);
+    cudaFree(u->sx);
+    cudaFree(u->st);
+    cudaFree(u->phi0);
+    for (void *p : u->fixed) cudaFree(p);
+    delete u;
+}
+
+bool unet_has_weights(const UNetState *u) { return u && u->have_weights; }
+float unet_kscale(const UNetState *u) { return u->kscale; }
+
+int unet_set_params(UNetState *u, const float *compact, int n, float kscale, cudaStream_t s)
+{
+    if (n != NPARAM || !compact || !(kscale > 0.f)) return HC_ERR_ARG;
+    std::vector<float> f;
+    compact_to_full(compact, f);
+    if (cudaMemcpyAsync(u->pm, f.data(), (size_t)NFULL * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return HC_ERR_CUDA;
+    cudaMemsetAsync(u->am, 0, (size_t)2 * NFULL * 4, s);   // am, av adjacent
+    u->adam_t = 0;
+    u->kscale = kscale;
+    if (pack_all(u, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HC_ERR_CUDA;
+    u->have_weights = true;
+    return HC_OK;
+}
+
+int unet_get_params(UNetState *u, float *compact, int n, cudaStream_t s)
+{
+    if (n != NPARAM || !compact) return HC_ERR_ARG;
+    std::vector<float> f(NFULL);
+    if (cudaMemcpyAsync(f.data(), u->pm, (size_t)NFULL * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HC_ERR_CUDA;
+    full_to_compact(f, compact);
+    return HC_OK;
+}
+
+// uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights and biases
+int unet_init(UNetState *u, unsigned seed, cudaStream_t s)
+{
+    std::mt19937 rng(seed);
+    std::vector<float> c(NPARAM);
+    size_t q = 0;
+    for (int l = 0; l < NCONV; l++) {
+        const int fan = NTAP * (l == 0 ? 1 : CH);
+        const float b = 1.f / std::sqrt((float)fan);
+        std::uniform_real_distribution<float> U(-b, b);
+        const int nw = (l == 0 || l == NCONV - 1) ? CH * NTAP : WELEM;
+        const int nb = (l == NCONV - 1) ? 1 : CH;
+        for (int t = 0; t < nw + nb; t++) c[q++] = U(rng);
+    }
+    return unet_set_params(u, c.data(), NPARAM, 30.f, s);
+}
+
+int unet_collect(UNetState *u, int capacity)
+{
+    if (capacity < 0) return HC_ERR_ARG;
+    cudaFree(u->sx);
+    cudaFree(u->st);
+    u->sx = u->st = nullptr;
+    u->cap = capacity;
+    u->count = u->next = 0;
+    u->slot = -1;
+    u->st2.assign(capacity, 0.0);
+    if (capacity > 0 && u->gx) {
+        if (dalloc((void **)&u->sx, (size_t)capacity * u->L[0].n * 4) ||
+            dalloc((void **)&u->st, (size_t)capacity * u->L[0].n * 4))
+            return HC_ERR_NOMEM;
+    }
+    return HC_OK;
+}
+
+int unet_samples(const UNetState *u) { return u ? u->count : 0; }
+bool unet_collecting(const UNetState *u) { return u && u->cap > 0; }
+
+// At the start of a mixed-precision solve, after the first FP64 residual
+// (r32, colour split): prepare the network input and, when `e_out` is given,
+// predict the correction into it (colour split, zero on boundary cells).
+// When collecting, also record the input and a copy of phi for the target.
+int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e_out, cudaStream_t s)
+{
+    int rc = ensure_grid(u, a.g.nx, a.g.ny, a.g.nz);
+    if (rc) return rc;
+    const Split sp = make_split(a.g);
+    cudaMemsetAsync(u->scal, 0, sizeof(double), s);
+    in_pool_kernel<<<nblk(u->L[0].n), 256, 0, s>>>(r32, sp, u->L[0], u->pooled, u->scal);
+    const bool collect = u->cap > 0 && u->sx;
+    u->slot = collect ? u->next : -1;
+    float *xs = collect ? u->sx + (size_t)u->slot * u->L[0].n : nullptr;
+    in_norm_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->pooled, u->scal, u->L[0].n, u->x0, xs);
+    if (collect) {
+        if (u->phi0_n != a.g.n) {
+            cudaFree(u->phi0);
+            if (dalloc((void **)&u->phi0, (size_t)a.g.n * 8)) return HC_ERR_NOMEM;
+            u->phi0_n = a.g.n;
+        }
+        cudaMemcpyAsync(u->phi0, a.phi, (size_t)a.g.n * 8, cudaMemcpyDeviceToDevice, s);
+    }
+    if (e_out) {
+        if (!u->have_weights) return HC_ERR_STATE;
+        if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+        out_up_kernel<<<nblk(a.g.n), 256, 0, s>>>(u->out0, u->L[0], u->scal, u->kscale, sp, e_out);
+    }
+    return cudaGetLastError() == cudaSuccess ? HC_OK : HC_ERR_CUDA;
+}
+
+// At the end of a converged solve: the recorded sample's target.
+int unet_end_solve(UNetState *u, const GravArgs &a, bool converged, cudaStream_t s)
+{
+    if (u->slot < 0) return HC_OK;
+    const int slot = u->slot;
+    u->slot = -1;
+    if (!converged) return HC_OK;
+    cudaMemsetAsync(u->scal + 1, 0, sizeof(double), s);
+    target_kernel<<<nblk(u->L[0].n), 256, 0, s>>>(a.phi, u->phi0, a.g, u->L[0], u->scal, u->kscale,
+                                                  u->st + (size_t)slot * u->L[0].n, u->scal + 1);
+    double t2 = 0.0;
+    if (cudaMemcpyAsync(&t2, u->scal + 1, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HC_ERR_CUDA;
+    if (!(t2 > 0.0)) return HC_OK;   // nothing to learn from a zero correction
+    u->st2[slot] = t2;
+    u->next = (u->next + 1) % u->cap;
+    u->count = std::min(u->count + 1, u->cap);
+    return HC_OK;
+}
+
+// `steps` Adam steps (learning rate decayed from lr to 0 on a cosine), each on
+// one stored sample (a seeded random order); mean loss of the last quarter
+int unet_train(UNetState *u, int steps, double lr, unsigned seed, double *mean_loss, cudaStream_t s)
+{
+    if (steps < 0 || !(lr > 0.0)) return HC_ERR_ARG;
+    if (u->count == 0) return HC_ERR_STATE;
+    std::mt19937 rng(seed);
+    const long long n0 = u->L[0].n;
+    double acc = 0.0;
+    int nacc = 0;
+    const int tail = std::max(1, steps / 4);
+    cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
+    for (int k = 0; k < steps; k++) {
+        const int smp = (int)(rng() % (unsigned)u->count);
+        in_expand_kernel<<<nblk(n0 * 2), 256, 0, s>>>(u->sx + (size_t)smp * n0, n0, u->x0);
+        if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+        if (k == steps - tail) cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
+        if (loss_grad(u, u->st + (size_t)smp * n0, u->st2[smp], s) != cudaSuccess) return HC_ERR_CUDA;
+        if (backward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+        // cosine decay of the learning rate over this call's steps
+        const double lrk = lr * 0.5 * (1.0 + std::cos(3.14159265358979 * k / std::max(1, steps)));
+        if (adam_step(u, (float)lrk, s) != cudaSuccess) return HC_ERR_CUDA;
+        if (k >= steps - tail) nacc++;
+    }
+    int rc = read_err(u, s);
+    if (rc) return rc;
+    if (cudaMemcpyAsync(&acc, u->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HC_ERR_CUDA;
+    u->have_weights = true;
+    if (mean_loss) *mean_loss = nacc ? acc / nacc : 0.0;
+    return HC_OK;
+}
+
+// One forward + backward on host data at level-0 dims (x: normalised input,
+// t: target, n0 values each): the loss and the compact gradient.
+int unet_loss_grad(UNetState *u, int n0x, int n0y, int n0z, const float *x, const float *t, double *loss,
+                   float *grad, float *out, cudaStream_t s)
+{
+    int rc = ensure_grid(u, 2 * n0x, 2 * n0y, 2 * n0z);
+    if (rc) return rc;
+    const long long n0 = u->L[0].n;
+    float *dx = u->pooled, *dt = u->xnorm;   // free level-0 FP32 buffers
+    cudaMemcpyAsync(dx, x, n0 * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dt, t, n0 * 4, cudaMemcpyHostToDevice, s);
+    double t2 = 0.0;
+    for (long long v = 0; v < n0; v++) t2 += (double)t[v] * t[v];
+    in_expand_kernel<<<nblk(n0 * 2), 256, 0, s>>>(dx, n0, u->x0);
+    if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+    cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
+    cudaMemsetAsync(u->pg, 0, (size_t)NFULL * 4, s);
+    if (loss_grad(u, dt, t2, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (backward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+    rc = read_err(u, s);
+    if (rc) return rc;
+    std::vector<float> g(NFULL);
+    cudaMemcpyAsync(g.data(), u->pg, (size_t)NFULL * 4, cudaMemcpyDeviceToHost, s);
+    if (out) cudaMemcpyAsync(out, u->out0, n0 * 4, cudaMemcpyDeviceToHost, s);
+    if (loss) cudaMemcpyAsync(loss, u->scal + 2, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HC_ERR_CUDA;
+    if (grad) full_to_compact(g, grad);
+    return HC_OK;
+}
+
 }  // namespace hc
 
 using namespace hc;

@@ -107,6 +107,9 @@ typedef struct hc_diag {
     long long steps;         /* steps taken by this context */
     long long total_iterations;
     int overshoot;           /* temporal blocking crossed tol inside a pass */
+    long long unet_accepted; /* solves that started from the learned prediction */
+    long long unet_fallbacks;/* solves whose prediction was rejected (larger FP64
+                                residual than the previous potential's) */
 } hc_diag;
 
 /* Per-kernel-family device time (CUDA events on the context's stream),
@@ -174,10 +177,38 @@ int hc_sync(hc_ctx *ctx);
 int hc_timer_start(hc_ctx *ctx);
 int hc_timer_stop(hc_ctx *ctx, double *ms);
 
-/* Learned warm start: load weights (nparam BF16 values as uint16) or query
- * the parameter count of the network built into this library. */
+/* Learned warm start (no reference counterpart).  A 3D U-Net (16 channels, 3
+ * pooling levels, LeakyReLU, 49,377 parameters; BF16 weights and activations,
+ * FP32 accumulation on the tensor cores) maps the first FP64 residual of a
+ * mixed-precision solve (HC_FP32, colour-split sweeps, grid dimensions
+ * multiples of 16) to a correction of the previous potential:
+ *   e0 = trilinear_up(net(pool2(delta) / rms)) * rms * kscale.
+ * With warm_start = HC_WARM_UNET the solve starts from phi + e0 when that
+ * lowers max|delta|, else from phi (counted in hc_diag); SOR then iterates to
+ * the same tolerance either way.
+ * Parameters: compact FP32 vector of hc_unet_param_count() values (per conv:
+ * weights [co][tap][ci] then biases; the first conv has one input channel,
+ * the last one output channel).  Files: "HCUNET01", int32 count, float32
+ * kscale, float32 parameters.
+ * Training on the device: hc_unet_collect(ctx, capacity) records one
+ * (normalised residual, normalised converged correction) pair per
+ * mixed-precision solve into a ring; hc_unet_train runs `steps` Adam steps
+ * (lr, seeded sample order) of the relative squared error and returns the
+ * mean loss of the last quarter of the steps.  hc_unet_loss_grad: one forward
+ * and backward pass on host data at the network's level-0 dimensions (each a
+ * multiple of 8; x normalised input, t target, nx*ny*nz values): loss, the
+ * compact gradient and the output (each nullable). */
 int hc_unet_param_count(void);
-int hc_unet_load(hc_ctx *ctx, const uint16_t *w_bf16, int nparam);
+int hc_unet_init(hc_ctx *ctx, unsigned seed);
+int hc_unet_load(hc_ctx *ctx, const float *params, int nparam, double kscale);
+int hc_unet_save(hc_ctx *ctx, float *params, int nparam, double *kscale);
+int hc_unet_load_file(hc_ctx *ctx, const char *path);
+int hc_unet_save_file(hc_ctx *ctx, const char *path);
+int hc_unet_collect(hc_ctx *ctx, int capacity);
+int hc_unet_samples(hc_ctx *ctx);
+int hc_unet_train(hc_ctx *ctx, int steps, double lr, unsigned seed, double *mean_loss);
+int hc_unet_loss_grad(hc_ctx *ctx, int nx, int ny, int nz, const float *x, const float *t, double *loss,
+                      float *grad, float *out);
 
 /* Diagnostics of the tensor-core convolution kernels (no reference
  * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16
