@@ -51,11 +51,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", default="best", choices=["best", "fp32", "fp64", "fp64_tree"])
+    ap.add_argument("--variant", default="best", choices=["best", "fp32_unet", "fp32", "fp64", "fp64_tree"])
     ap.add_argument("--n", type=int, default=256, help="grid cells per side")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-fp32-compare", action="store_true",
+                    help="skip the FP32 arm without the learned warm start")
     return ap.parse_args()
 
 
@@ -150,15 +152,30 @@ def solver_kwargs(p, variant, device):
         kw.update(precision=hc.FP64, lmax=p["lmax"], moment_order=hc.MOMENTS_TREE)
     elif variant == "fp64_tree":
         kw.update(precision=hc.FP64, moment_order=hc.MOMENTS_TREE)
+    elif variant == "fp32_unet":
+        kw.update(precision=hc.FP32, moment_order=hc.MOMENTS_TREE, warm_start=hc.HC_WARM_UNET)
     else:
         kw.update(precision=hc.FP32, moment_order=hc.MOMENTS_TREE)
     return kw
 
 
-def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
-    """Warm up, then time `steps` steps with CUDA events on the solver's stream."""
+# Weights of the warm-start U-Net, trained on the GPU by
+# `python -m hydrocode_astro1_b200.train_unet` from solves of this workload
+# with another density-noise seed (7); the benchmark run uses seed 42.
+UNET_WEIGHTS = os.path.join(ROOT, "hydrocode_astro1_b200", "data", "unet_stellar_explosion_256.bin")
+
+
+def make_solver(p, variant, device):
     import hydrocode_astro1_b200 as hc
     s = hc.HydroSolver3D(p["shape"], **solver_kwargs(p, variant, device))
+    if variant == "fp32_unet":
+        s.unet_load_file(UNET_WEIGHTS)
+    return s
+
+
+def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
+    """Warm up, then time `steps` steps with CUDA events on the solver's stream."""
+    s = make_solver(p, variant, device)
     s.set_state(q0)
     warm_iters = []
     for w in range(warmup):
@@ -168,6 +185,7 @@ def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
         log(f"[bench] {variant} warm-up step {w}: {time.perf_counter() - t:.3f} s, "
             f"{warm_iters[-1]} SOR iterations")
     warm_launches = s.timing(reset=True)["launches"]
+    diag0 = s.diagnostics()
     iters = []
     barrier(dist)
     s.sync()
@@ -190,7 +208,8 @@ def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
     tm = s.timing()
     d = s.diagnostics()
     return dict(solver=s, ms=ms, iters=iters, warm_iters=warm_iters, timing=tm, diag=d,
-                dts=dts, clocks=ck, total_iters=d["total_iterations"] - d0, warm_launches=warm_launches)
+                dts=dts, clocks=ck, total_iters=d["total_iterations"] - d0, warm_launches=warm_launches,
+                diag0=diag0)
 
 
 def nvtx_mod():
@@ -324,7 +343,9 @@ def main_ours(args):
 
     import hydrocode_astro1_b200 as hc
     world, rank, local, dist = dist_setup(args)
-    variant = "fp32" if args.variant == "best" else args.variant
+    variant = args.variant
+    if variant == "best":
+        variant = "fp32_unet" if (args.n == 256 and os.path.exists(UNET_WEIGHTS)) else "fp32"
     q0, p = make_workload(args.n)
     ncell = p["shape"][0] * p["shape"][1] * p["shape"][2]
     clocks = Clocks(local)
@@ -365,7 +386,8 @@ def main_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if fp64 else "f32 hydro / f64+f32 poisson",
+        "dtype": "f64" if fp64 else ("f32 hydro / f64+f32 poisson / bf16 u-net" if variant == "fp32_unet"
+                                     else "f32 hydro / f64+f32 poisson"),
         "data": "synthetic",
         "config": {"workload": f"stellar_explosion_{args.n}^3 (n=3 star, lmax 8, tol 1e-8)",
                    "grid": list(p["shape"]), "variant": variant,
@@ -381,10 +403,39 @@ def main_ours(args):
         "clocks": r["clocks"],
     }
 
+    def poisson_ms(t, k):
+        return (t["sor_ms"] + t["residual_ms"] + t["moments_ms"] + t["unet_ms"]) / k
+
+    # the same FP32 path without the learned warm start
+    if variant == "fp32_unet" and not args.no_fp32_compare:
+        qmain = s.state()
+        s.close()
+        rp = run_variant(q0, p, "fp32", args.steps, args.warmup, local, dist, None)
+        msp = reduce_max(dist, rp["ms"])
+        d1, dd0 = r["diag"], r["diag0"]
+        line["fp32_plain"] = {"value": ncell * args.steps * world / (msp / 1e3) / 1e6,
+                              "ms_per_step": msp / args.steps, "sor_iterations_per_step": rp["iters"]}
+        line["learned_warm_start"] = {
+            "weights": os.path.relpath(UNET_WEIGHTS, ROOT),
+            "accepted": d1["unet_accepted"] - dd0["unet_accepted"],
+            "fallbacks": d1["unet_fallbacks"] - dd0["unet_fallbacks"],
+            "sor_iterations_learned": r["iters"], "sor_iterations_plain": rp["iters"],
+            "iterations_saved_frac": 1.0 - sum(r["iters"]) / max(1, sum(rp["iters"])),
+            "poisson_ms_per_solve_learned": poisson_ms(tm, args.steps),
+            "poisson_ms_per_solve_plain": poisson_ms(rp["timing"], args.steps),
+            "unet_ms_per_solve": tm["unet_ms"] / args.steps,
+            "density_l1_vs_plain": float(np.abs(qmain[0] - rp["solver"].state()[0]).mean()
+                                         / np.abs(rp["solver"].state()[0]).mean())}
+        rp["solver"].close()
+        s = None
+
     # the plain FP64 path on the same workload, for the FP32/FP64 speed-up
     if not fp64 and not args.no_fp64_compare:
-        q32 = s.state()
-        s.close()
+        if s is None:
+            q32 = qmain
+        else:
+            q32 = s.state()
+            s.close()
         r64 = run_variant(q0, p, "fp64", args.steps, args.warmup, local, dist, None)
         ms64 = reduce_max(dist, r64["ms"])
         v64 = ncell * args.steps * world / (ms64 / 1e3) / 1e6
@@ -408,7 +459,13 @@ def main_ours(args):
             "time_fp32": float(sum(r["dts"]) + 0.0), "time_fp64": float(sum(r64["dts"]))}
         del q32, q64
         r64["solver"].close()
-        s = hc.HydroSolver3D(p["shape"], **solver_kwargs(p, variant, local))
+        s = make_solver(p, variant, local)
+        s.set_state(q0)
+        for _ in range(args.warmup):
+            s.step(1)
+
+    if s is None:   # the main solver was closed for a comparison arm
+        s = make_solver(p, variant, local)
         s.set_state(q0)
         for _ in range(args.warmup):
             s.step(1)
