@@ -25,9 +25,7 @@ namespace {
 
 constexpr int LM_MAX = 12;
 constexpr int LM_NC = (LM_MAX + 1) * (LM_MAX + 1);
-constexpr int MOM_CH = 64;        // cells per chunk
-constexpr int MOM_NT = 192;       // >= LM_NC threads
-constexpr int MOM_NB = 296;
+constexpr int MOM_NB = 148;      // blocks of the moment reduction (one per SM)
 
 __constant__ double c_norm[LM_NC];   // N_lm at l*(LM_MAX+1)+m
 
@@ -65,44 +63,85 @@ __device__ __forceinline__ void solid_harmonics(double x, double y, double z, in
     }
 }
 
-__global__ void __launch_bounds__(MOM_NT) lmax_partial(GravArgs a, const double *com)
+__constant__ double c_rinv[LM_MAX + 1];   // 1 / d for d = l - m >= 2 (index d)
+
+// Solid-harmonic moments, one order m per warp: lane L of warp m takes the
+// cells L, L + 32*gridDim, ... and accumulates, in registers, dm N_lm Q_l^m
+// for l = m..lmax with the recursion of solid_harmonics (same operations, the
+// division by l-m replaced by the identical product with 1/(l-m) computed on
+// the host); a fixed butterfly reduction per warp writes this block's partial
+// sums, which lmax_final adds in block order.
+__global__ void __launch_bounds__(32 * (LM_MAX + 1)) lmax_partial(GravArgs a, const double *com)
 {
-    extern __shared__ double tile[];          // nc x MOM_CH
     const Geom g = a.g;
-    const int nc = (a.lmax + 1) * (a.lmax + 1);
+    const int lmax = a.lmax;
+    const int m = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (m > lmax) return;
     const double dV = g.dx * g.dy * g.dz;
     const long long sjk = (long long)g.ny * g.nz, snz = g.nz;
     const double xc = com[0], yc = com[1], zc = com[2];
-    double acc = 0.0;   // thread t < nc owns coefficient t
-    for (long long base = (long long)blockIdx.x * MOM_CH; base < g.n;
-         base += (long long)gridDim.x * MOM_CH) {
-        if (threadIdx.x < MOM_CH) {
-            const int e = threadIdx.x;
-            long long c = base + e;
-            double r = 0.0;
-            if (c < g.n) r = a.rho ? a.rho[c] : (double)a.rho32[c];
-            if (r > 0.0) {
-                int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
-                double x = g.xmin + (i + 0.5) * g.dx - xc;
-                double y = g.ymin + (j + 0.5) * g.dy - yc;
-                double z = g.zmin + (k + 0.5) * g.dz - zc;
-                double dm = r * dV;
-                solid_harmonics(x, y, z, a.lmax, [&](int t, double v) { tile[t * MOM_CH + e] = dm * v; });
+    double ar[LM_MAX + 1], ai[LM_MAX + 1];
+#pragma unroll
+    for (int d = 0; d <= LM_MAX; d++) ar[d] = ai[d] = 0.0;
+    for (long long c = (long long)blockIdx.x * 32 + lane; c < g.n; c += (long long)gridDim.x * 32) {
+        const double r = a.rho ? a.rho[c] : (double)a.rho32[c];
+        if (!(r > 0.0)) continue;
+        const int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
+        const double x = g.xmin + (i + 0.5) * g.dx - xc;
+        const double y = g.ymin + (j + 0.5) * g.dy - yc;
+        const double z = g.zmin + (k + 0.5) * g.dz - zc;
+        const double dm = r * dV;
+        const double r2 = x * x + y * y + z * z;
+        double smr = 1.0, smi = 0.0;      // Q_m^m
+        for (int q = 1; q <= m; q++) {
+            const double f = (double)(2 * q - 1);
+            const double nr = f * (x * smr - y * smi);
+            const double ni = f * (x * smi + y * smr);
+            smr = nr;
+            smi = ni;
+        }
+        double pr = smr, pi = smi, ppr = 0.0, ppi = 0.0;
+        {
+            const double nrm = c_norm[m * (LM_MAX + 1) + m];
+            ar[0] += dm * (nrm * smr);
+            ai[0] += dm * (nrm * smi);
+        }
+#pragma unroll
+        for (int d = 1; d <= LM_MAX; d++) {
+            const int l = m + d;
+            if (l > lmax) break;
+            double cr, ci;
+            if (d == 1) {
+                cr = (2 * m + 1) * z * smr;
+                ci = (2 * m + 1) * z * smi;
             } else {
-                for (int t = 0; t < nc; t++) tile[t * MOM_CH + e] = 0.0;
+                const double aa = (double)(2 * l - 1), bb = (double)(l + m - 1), inv = c_rinv[d];
+                cr = (aa * z * pr - bb * r2 * ppr) * inv;
+                ci = (aa * z * pi - bb * r2 * ppi) * inv;
             }
+            ppr = pr;
+            ppi = pi;
+            pr = cr;
+            pi = ci;
+            const double nrm = c_norm[l * (LM_MAX + 1) + m];
+            ar[d] += dm * (nrm * cr);
+            ai[d] += dm * (nrm * ci);
         }
-        __syncthreads();
-        if (threadIdx.x < nc) {
-            const double *tt = tile + threadIdx.x * MOM_CH;
-            double s = 0.0;
-#pragma unroll 8
-            for (int e = 0; e < MOM_CH; e++) s += tt[e];
-            acc += s;
-        }
-        __syncthreads();
     }
-    if (threadIdx.x < nc) a.scratch[(long long)blockIdx.x * LM_NC + threadIdx.x] = acc;
+#pragma unroll
+    for (int d = 0; d <= LM_MAX; d++) {
+        double vr = ar[d], vi = ai[d];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            vr += __shfl_xor_sync(0xffffffffu, vr, o);
+            vi += __shfl_xor_sync(0xffffffffu, vi, o);
+        }
+        const int l = m + d;
+        if (lane == 0 && l <= lmax) {
+            a.scratch[(long long)blockIdx.x * LM_NC + l * l + l + m] = vr;
+            if (m > 0) a.scratch[(long long)blockIdx.x * LM_NC + l * l + l - m] = vi;
+        }
+    }
 }
 
 __global__ void lmax_final(GravArgs a)
@@ -178,6 +217,10 @@ cudaError_t ensure_norm()
             h[l * (LM_MAX + 1) + m] = v;
         }
     cudaError_t e = cudaMemcpyToSymbol(c_norm, h, sizeof h);
+    if (e != cudaSuccess) return e;
+    double rinv[LM_MAX + 1];
+    for (int d = 0; d <= LM_MAX; d++) rinv[d] = d > 0 ? 1.0 / (double)d : 0.0;
+    e = cudaMemcpyToSymbol(c_rinv, rinv, sizeof rinv);
     if (e == cudaSuccess && dev < 64) g_norm_ready[dev] = true;
     return e;
 }
@@ -194,16 +237,7 @@ cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
     GravArgs t = a;
     e = grav_moments_tree(t, s);       // M, COM, Q (Q unused here)
     if (e != cudaSuccess) return e;
-    const int nc = lmax_ncoef(a.lmax);
-    const size_t sm = (size_t)nc * MOM_CH * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        e = cudaFuncSetAttribute(lmax_partial, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)(LM_NC * MOM_CH * sizeof(double)));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    lmax_partial<<<MOM_NB, MOM_NT, sm, s>>>(a, a.sc->moments + 1);
+    lmax_partial<<<MOM_NB, 32 * (a.lmax + 1), 0, s>>>(a, a.sc->moments + 1);
     lmax_final<<<1, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
