@@ -25,7 +25,6 @@ namespace {
 
 constexpr int LM_MAX = 12;
 constexpr int LM_NC = (LM_MAX + 1) * (LM_MAX + 1);
-constexpr int MOM_NB = 148;      // blocks of the moment reduction (one per SM)
 
 __constant__ double c_norm[LM_NC];   // N_lm at l*(LM_MAX+1)+m
 
@@ -65,30 +64,35 @@ __device__ __forceinline__ void solid_harmonics(double x, double y, double z, in
 
 __constant__ double c_rinv[LM_MAX + 1];   // 1 / d for d = l - m >= 2 (index d)
 
-// Solid-harmonic moments, one order m per warp: lane L of warp m takes the
-// cells L, L + 32*gridDim, ... and accumulates, in registers, dm N_lm Q_l^m
+// Solid-harmonic moments, one order m per warp: block b takes the (i,j) rows
+// b, b + gridDim, ..., lane L the cells k = L, L+32, ... of each row, and
+// accumulates, in registers, dm N_lm Q_l^m
 // for l = m..lmax with the recursion of solid_harmonics (same operations, the
 // division by l-m replaced by the identical product with 1/(l-m) computed on
 // the host); a fixed butterfly reduction per warp writes this block's partial
 // sums, which lmax_final adds in block order.
-__global__ void __launch_bounds__(32 * (LM_MAX + 1)) lmax_partial(GravArgs a, const double *com)
+template <int LMAX>
+__global__ void __launch_bounds__(32 * (LMAX + 1)) lmax_partial(GravArgs a, const double *com)
 {
     const Geom g = a.g;
-    const int lmax = a.lmax;
+    constexpr int lmax = LMAX;
     const int m = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (m > lmax) return;
     const double dV = g.dx * g.dy * g.dz;
-    const long long sjk = (long long)g.ny * g.nz, snz = g.nz;
+    const long long snz = g.nz;
     const double xc = com[0], yc = com[1], zc = com[2];
-    double ar[LM_MAX + 1], ai[LM_MAX + 1];
+    double ar[LMAX + 1], ai[LMAX + 1];
 #pragma unroll
-    for (int d = 0; d <= LM_MAX; d++) ar[d] = ai[d] = 0.0;
-    for (long long c = (long long)blockIdx.x * 32 + lane; c < g.n; c += (long long)gridDim.x * 32) {
+    for (int d = 0; d <= LMAX; d++) ar[d] = ai[d] = 0.0;
+    const long long rows = (long long)g.nx * g.ny;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+      const int i = (int)(row / g.ny), j = (int)(row % g.ny);
+      const double x = g.xmin + (i + 0.5) * g.dx - xc;
+      const double y = g.ymin + (j + 0.5) * g.dy - yc;
+      for (int k = lane; k < g.nz; k += 32) {
+        const long long c = row * snz + k;
         const double r = a.rho ? a.rho[c] : (double)a.rho32[c];
         if (!(r > 0.0)) continue;
-        const int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
-        const double x = g.xmin + (i + 0.5) * g.dx - xc;
-        const double y = g.ymin + (j + 0.5) * g.dy - yc;
         const double z = g.zmin + (k + 0.5) * g.dz - zc;
         const double dm = r * dV;
         const double r2 = x * x + y * y + z * z;
@@ -107,7 +111,7 @@ __global__ void __launch_bounds__(32 * (LM_MAX + 1)) lmax_partial(GravArgs a, co
             ai[0] += dm * (nrm * smi);
         }
 #pragma unroll
-        for (int d = 1; d <= LM_MAX; d++) {
+        for (int d = 1; d <= LMAX; d++) {
             const int l = m + d;
             if (l > lmax) break;
             double cr, ci;
@@ -127,9 +131,10 @@ __global__ void __launch_bounds__(32 * (LM_MAX + 1)) lmax_partial(GravArgs a, co
             ar[d] += dm * (nrm * cr);
             ai[d] += dm * (nrm * ci);
         }
+      }
     }
 #pragma unroll
-    for (int d = 0; d <= LM_MAX; d++) {
+    for (int d = 0; d <= LMAX; d++) {
         double vr = ar[d], vi = ai[d];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -144,12 +149,12 @@ __global__ void __launch_bounds__(32 * (LM_MAX + 1)) lmax_partial(GravArgs a, co
     }
 }
 
-__global__ void lmax_final(GravArgs a)
+__global__ void lmax_final(GravArgs a, int nparts)
 {
     const int nc = (a.lmax + 1) * (a.lmax + 1);
     for (int t = threadIdx.x; t < nc; t += blockDim.x) {
         double s = 0.0;
-        for (int b = 0; b < MOM_NB; b++) s += a.scratch[(long long)b * LM_NC + t];
+        for (int b = 0; b < nparts; b++) s += a.scratch[(long long)b * LM_NC + t];
         a.mom[4 + t] = s;
     }
     if (threadIdx.x == 0) {
@@ -231,14 +236,43 @@ cudaError_t ensure_norm()
 cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
 {
     if (a.lmax < 1 || a.lmax > LM_MAX) return cudaErrorInvalidValue;
-    if (a.scratch_len < (long long)MOM_NB * LM_NC) return cudaErrorInvalidValue;
+
     cudaError_t e = ensure_norm();
     if (e != cudaSuccess) return e;
     GravArgs t = a;
     e = grav_moments_tree(t, s);       // M, COM, Q (Q unused here)
     if (e != cudaSuccess) return e;
-    lmax_partial<<<MOM_NB, 32 * (a.lmax + 1), 0, s>>>(a, a.sc->moments + 1);
-    lmax_final<<<1, 256, 0, s>>>(a);
+    // blocks: every SM filled to its occupancy for this l_max
+    static int nb_cache[LM_MAX + 1] = { 0 };
+    int nb = nb_cache[a.lmax];
+    auto launch = [&](auto kern) -> cudaError_t {
+        if (!nb) {
+            int per = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * (a.lmax + 1), 0) != cudaSuccess ||
+                per < 1)
+                per = 1;
+            nb = std::min(148 * per, (int)(a.scratch_len / LM_NC));
+            nb_cache[a.lmax] = nb;
+        }
+        kern<<<nb, 32 * (a.lmax + 1), 0, s>>>(a, a.sc->moments + 1);
+        return cudaGetLastError();
+    };
+    switch (a.lmax) {
+    case 1: e = launch(lmax_partial<1>); break;
+    case 2: e = launch(lmax_partial<2>); break;
+    case 3: e = launch(lmax_partial<3>); break;
+    case 4: e = launch(lmax_partial<4>); break;
+    case 5: e = launch(lmax_partial<5>); break;
+    case 6: e = launch(lmax_partial<6>); break;
+    case 7: e = launch(lmax_partial<7>); break;
+    case 8: e = launch(lmax_partial<8>); break;
+    case 9: e = launch(lmax_partial<9>); break;
+    case 10: e = launch(lmax_partial<10>); break;
+    case 11: e = launch(lmax_partial<11>); break;
+    default: e = launch(lmax_partial<12>); break;
+    }
+    if (e != cudaSuccess) return e;
+    lmax_final<<<1, 256, 0, s>>>(a, nb);
     return cudaGetLastError();
 }
 
