@@ -500,6 +500,28 @@ static int grav_moments(hc_ctx *c, const GravArgs &a)
     return HC_OK;
 }
 
+// Iterations to queue before the next host poll of an SOR solve: from the
+// update norms of the last polled iterations (slots[0..nb)), the geometric
+// rate r over up to 32 iterations predicts the iterations left to reach
+// thresh; queue 10% more plus two, between 8 and 512.  Without a usable
+// rate, double the previous batch (at most 256).  Queued sweeps past the stop
+// only cost early-exit launches, so the prediction trades those against polls.
+static int next_batch(const double *slots, int nb, double thresh, int prev)
+{
+    int w = std::min(32, nb - 1);
+    while (w >= 4 && !(slots[nb - 1 - w] > 0.0)) w /= 2;
+    const double last = slots[nb - 1];
+    if (w >= 4 && last > 0.0 && slots[nb - 1 - w] > last) {
+        const double rate = std::pow(last / slots[nb - 1 - w], 1.0 / w);
+        if (rate > 0.0 && rate < 0.9999) {
+            const double rem = std::log(thresh / last) / std::log(rate);
+            if (rem <= 0.0) return 8;
+            return (int)std::min(512.0, std::max(8.0, 1.1 * rem + 2.0));
+        }
+    }
+    return std::min(prev * 2, 256);
+}
+
 // Red-black SOR to tolerance, FP64 (gravity_solve_potential,
 // gravity_solver_3d.c:510-747).  Returns 0 / -1 like the reference, or a
 // negative HC_ERR_* code.
@@ -593,13 +615,17 @@ static int sor_fp64(hc_ctx *c, const double *rho)
         }
         c->launches += 1;
         CK(cudaMemcpyAsync(&c->hsc->done, &c->sc->done, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->s));
+        const int nb = std::min(end - it, 512);
+        if (!c->hslots && cudaMallocHost((void **)&c->hslots, 512 * sizeof(double)) != cudaSuccess)
+            return set_err(HC_ERR_NOMEM, "pinned slot buffer");
+        CK(cudaMemcpyAsync(c->hslots, c->res + (end - nb), nb * sizeof(double), cudaMemcpyDeviceToHost, c->s));
         rc = sync_ctx(c);
         if (rc) return rc;
         done = c->hsc->done;
         last = c->hsc->last_iter;
         if (done || end >= a.max_iter) break;
         it = end;
-        batch = std::min(batch * 2, 256);
+        batch = next_batch(c->hslots, nb, a.tol, batch);
     }
     int used = done ? last : a.max_iter;
     if (wave && (used & 1)) std::swap(c->phi, c->phi2);   // result in buf[used % 2]
@@ -766,7 +792,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
                 break;
             }
             it = end;
-            batch = std::min(batch * 2, 256);
+            batch = next_batch(c->hslots, nb, thresh, batch);
         }
         const int used = done ? last : processed;
         total += used;
