@@ -695,7 +695,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
                     rc = unet_begin_solve(c->unet, a, c->r32, predict ? c->e32b : nullptr, c->s);
                     c->launches += predict ? 40 : 3;
                 }
-                if (rc) return set_err(rc, "learned warm start: grid dimensions must be multiples of 16");
+                if (rc) return set_err(rc, "learned warm start: grid dimensions must be multiples of 32");
                 recorded = unet_collecting(c->unet);
             }
             if (predict) {
@@ -1322,8 +1322,8 @@ extern "C" int hc_unet_train(hc_ctx *c, int steps, double lr, unsigned seed, dou
 extern "C" int hc_unet_loss_grad(hc_ctx *c, int nx, int ny, int nz, const float *x, const float *t, double *loss,
                                  float *grad, float *out)
 {
-    if (!c || !c->unet || !x || !t || nx < 2 || ny < 2 || nz < 2 || nx % 8 || ny % 8 || nz % 8)
-        return set_err(HC_ERR_ARG, "bad argument (level-0 dimensions must be multiples of 8)");
+    if (!c || !c->unet || !x || !t || nx < 2 || ny < 2 || nz < 2 || nx % 16 || ny % 16 || nz % 16)
+        return set_err(HC_ERR_ARG, "bad argument (level-0 dimensions must be multiples of 16)");
     CK(cudaSetDevice(c->dev));
     const int rc = unet_loss_grad(c->unet, nx, ny, nz, x, t, loss, grad, out, c->s);
     return rc ? set_err(rc, "U-Net loss/gradient failed") : HC_OK;

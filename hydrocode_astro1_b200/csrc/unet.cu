@@ -49,27 +49,26 @@ cudaError_t wgrad(const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *dw, fl
 }  // namespace hc
 
 // ---------------------------------------------------------------------------
-// The network: a 3D U-Net on the half-resolution grid of the solve.
+// The network: a 3D U-Net on the half-resolution grid of the solve, with
+// NLEV = 4 pooling levels (level l has grid / 2^(l+1) cells per side):
 //   x0 (channel 0 = 2x-pooled FP64 residual / its RMS)
-//   e0 = f(conv0 x0)                 level 0 (grid / 2)
-//   e1 = f(conv1 pool e0)            level 1
-//   e2 = f(conv2 pool e1)            level 2
-//   e3 = f(conv3 pool e2), b = f(conv4 e3)      level 3
-//   d2 = f(conv5 (up b + e2)), d1 = f(conv6 (up d2 + e1)), d0 = f(conv7 (up d1 + e0))
-//   out = conv8 d0 (channel 0)
+//   e0 = f(conv0 x0);  e_l = f(conv_l pool e_{l-1})          l = 1..NLEV
+//   d_l = f(conv_{2 NLEV - l} (up h + e_l)), h = e_NLEV then d_{l+1},  l = NLEV-1..0
+//   out = conv_{2 NLEV + 1} d0 (channel 0)
 // f = LeakyReLU(0.1); pool = 2x average; up = 2x nearest.  16 channels at
-// every level; 49,377 trainable parameters.  The correction of the solve is
-//   e = trilinear_up(out) * RMS(pooled residual) * kscale.
+// every level; 2 NLEV + 2 = 10 convolutions, 56,305 trainable parameters.
+// The correction of the solve is  e = trilinear_up(out) * RMS(pooled residual) * kscale.
 // ---------------------------------------------------------------------------
 #include "unet_ops.cuh"
 
 namespace hc {
 
 namespace unet {
-constexpr int NCONV = 9;
+constexpr int NLEV = 4;                           // pooling levels
+constexpr int NCONV = 2 * NLEV + 2;
 constexpr int PFULL = WELEM + CH;                 // weights + bias of one conv, full layout
 constexpr int NFULL = NCONV * PFULL;
-constexpr int NPARAM = (CH * NTAP + CH) + 7 * (WELEM + CH) + (NTAP * CH + 1);   // 49377
+constexpr int NPARAM = (CH * NTAP + CH) + (NCONV - 2) * (WELEM + CH) + (NTAP * CH + 1);   // 56305
 constexpr int MAX_PARTS = 148;
 }  // namespace unet
 
@@ -85,11 +84,12 @@ struct UNetState {
     __nv_bfloat16 *wf = nullptr, *wt = nullptr;    // NCONV x WELEM each
     // buffers for one grid size
     int gx = 0, gy = 0, gz = 0;
-    Dims L[4];
-    __nv_bfloat16 *x0, *e0, *s0, *d0, *g0a, *g0b;
-    __nv_bfloat16 *p1, *e1, *s1, *d1, *g1a, *g1b, *g1c;
-    __nv_bfloat16 *p2, *e2, *s2, *d2, *g2a, *g2b, *g2c;
-    __nv_bfloat16 *p3, *e3, *bb, *g3a, *g3b;
+    Dims L[NLEV + 1];
+    __nv_bfloat16 *x0;
+    // per level: encoder output e, its pooled input p (l >= 1), decoder input
+    // sum s and output d (l < NLEV), gradient buffers ga, gb (skip), gc
+    __nv_bfloat16 *e[NLEV + 1], *p[NLEV + 1], *sm[NLEV + 1], *d[NLEV + 1];
+    __nv_bfloat16 *ga[NLEV + 1], *gb[NLEV + 1], *gc[NLEV + 1];
     float *out0 = nullptr, *pooled = nullptr, *xnorm = nullptr, *partial = nullptr, *bpart = nullptr;
     double *scal = nullptr;       // [0] sumsq of the input, [1] sum t^2, [2] loss
     int *err = nullptr;
@@ -179,25 +179,32 @@ void free_grid(UNetState *u)
 // Buffers for a solve grid of gx x gy x gz cells (each a multiple of 16).
 int ensure_grid(UNetState *u, int gx, int gy, int gz)
 {
-    if (gx % 16 || gy % 16 || gz % 16) return HC_ERR_ARG;
+    constexpr int MULT = 2 << NLEV;   // every level has integer dims
+    if (gx % MULT || gy % MULT || gz % MULT) return HC_ERR_ARG;
     if (u->gx == gx && u->gy == gy && u->gz == gz) return HC_OK;
     free_grid(u);
-    for (int l = 0; l < 4; l++) {
+    size_t nbf = 0;
+    for (int l = 0; l <= NLEV; l++) {
         const int f = 2 << l;
         u->L[l] = Dims{ gx / f, gy / f, gz / f, (long long)(gx / f) * (gy / f) * (gz / f) };
+        nbf += (size_t)u->L[l].n * CH * (l == 0 ? 8 : 7);
     }
-    const size_t v0 = (size_t)u->L[0].n * CH, v1 = (size_t)u->L[1].n * CH, v2 = (size_t)u->L[2].n * CH,
-                 v3 = (size_t)u->L[3].n * CH;
-    const size_t nbf = 6 * v0 + 7 * v1 + 7 * v2 + 5 * v3;
     const size_t nf = 3 * (size_t)u->L[0].n + (size_t)MAX_PARTS * WG_MT * TM * CH + 148 * 16 * CH;
     const size_t bytes = nbf * 2 + nf * 4 + 4 * sizeof(double) + 256 * 4;
     if (dalloc(&u->act_mem, bytes)) return HC_ERR_NOMEM;
     char *p = (char *)u->act_mem;
     auto take_bf = [&](size_t n) { __nv_bfloat16 *r = (__nv_bfloat16 *)p; p += n * 2; return r; };
-    u->x0 = take_bf(v0); u->e0 = take_bf(v0); u->s0 = take_bf(v0); u->d0 = take_bf(v0); u->g0a = take_bf(v0); u->g0b = take_bf(v0);
-    u->p1 = take_bf(v1); u->e1 = take_bf(v1); u->s1 = take_bf(v1); u->d1 = take_bf(v1); u->g1a = take_bf(v1); u->g1b = take_bf(v1); u->g1c = take_bf(v1);
-    u->p2 = take_bf(v2); u->e2 = take_bf(v2); u->s2 = take_bf(v2); u->d2 = take_bf(v2); u->g2a = take_bf(v2); u->g2b = take_bf(v2); u->g2c = take_bf(v2);
-    u->p3 = take_bf(v3); u->e3 = take_bf(v3); u->bb = take_bf(v3); u->g3a = take_bf(v3); u->g3b = take_bf(v3);
+    for (int l = 0; l <= NLEV; l++) {
+        const size_t v = (size_t)u->L[l].n * CH;
+        if (l == 0) u->x0 = take_bf(v);
+        u->e[l] = take_bf(v);
+        u->p[l] = l ? take_bf(v) : nullptr;
+        u->sm[l] = take_bf(v);
+        u->d[l] = take_bf(v);
+        u->ga[l] = take_bf(v);
+        u->gb[l] = take_bf(v);
+        u->gc[l] = take_bf(v);
+    }
     auto take_f = [&](size_t n) { float *r = (float *)p; p += n * 4; return r; };
     u->out0 = take_f(u->L[0].n); u->pooled = take_f(u->L[0].n); u->xnorm = take_f(u->L[0].n);
     u->partial = take_f((size_t)MAX_PARTS * WG_MT * TM * CH);
@@ -245,61 +252,52 @@ cudaError_t forward(UNetState *u, cudaStream_t s)
 {
     const Dims *L = u->L;
     cudaError_t e;
-    if ((e = conv_fwd(u, 0, u->x0, u->e0, 0, 0, s))) return e;
-    pool2_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->e0, u->p1, L[1]);
-    if ((e = conv_fwd(u, 1, u->p1, u->e1, 1, 0, s))) return e;
-    pool2_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->e1, u->p2, L[2]);
-    if ((e = conv_fwd(u, 2, u->p2, u->e2, 2, 0, s))) return e;
-    pool2_kernel<<<nblk(L[3].n * 2), 256, 0, s>>>(u->e2, u->p3, L[3]);
-    if ((e = conv_fwd(u, 3, u->p3, u->e3, 3, 0, s))) return e;
-    if ((e = conv_fwd(u, 4, u->e3, u->bb, 3, 0, s))) return e;
-    up_add_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->bb, u->e2, u->s2, L[2]);
-    if ((e = conv_fwd(u, 5, u->s2, u->d2, 2, 0, s))) return e;
-    up_add_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->d2, u->e1, u->s1, L[1]);
-    if ((e = conv_fwd(u, 6, u->s1, u->d1, 1, 0, s))) return e;
-    up_add_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->d1, u->e0, u->s0, L[0]);
-    if ((e = conv_fwd(u, 7, u->s0, u->d0, 0, 0, s))) return e;
-    return conv_fwd(u, 8, u->d0, u->out0, 0, 2, s);
+    if ((e = conv_fwd(u, 0, u->x0, u->e[0], 0, 0, s))) return e;
+    for (int l = 1; l <= NLEV; l++) {
+        pool2_kernel<<<nblk(L[l].n * 2), 256, 0, s>>>(u->e[l - 1], u->p[l], L[l]);
+        if ((e = conv_fwd(u, l, u->p[l], u->e[l], l, 0, s))) return e;
+    }
+    const __nv_bfloat16 *h = u->e[NLEV];
+    for (int l = NLEV - 1; l >= 0; l--) {
+        up_add_kernel<<<nblk(L[l].n * 2), 256, 0, s>>>(h, u->e[l], u->sm[l], L[l]);
+        if ((e = conv_fwd(u, 2 * NLEV - l, u->sm[l], u->d[l], l, 0, s))) return e;
+        h = u->d[l];
+    }
+    return conv_fwd(u, NCONV - 1, u->d[0], u->out0, 0, 2, s);
 }
 
-// gradients of the loss whose output gradient is in g0a (channel 0)
+// gradients of the loss whose output gradient is in ga[0] (channel 0)
 cudaError_t backward(UNetState *u, cudaStream_t s)
 {
     const Dims *L = u->L;
     cudaError_t e;
-    // conv8 (no activation)
-    if ((e = conv_wgrad(u, 8, u->d0, u->g0a, 0, s))) return e;
-    if ((e = conv_dgrad(u, 8, u->g0a, u->g0b, 0, s))) return e;
-    act_back_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->g0b, u->d0, u->g0a, L[0].n);   // dz7
-    if ((e = conv_wgrad(u, 7, u->s0, u->g0a, 0, s))) return e;
-    if ((e = conv_dgrad(u, 7, u->g0a, u->g0b, 0, s))) return e;                         // ds0 (skip to e0)
-    downsum_act_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->g0b, u->d1, u->g1a, L[1]);   // dz6
-    if ((e = conv_wgrad(u, 6, u->s1, u->g1a, 1, s))) return e;
-    if ((e = conv_dgrad(u, 6, u->g1a, u->g1b, 1, s))) return e;                         // ds1 (skip to e1)
-    downsum_act_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->g1b, u->d2, u->g2a, L[2]);   // dz5
-    if ((e = conv_wgrad(u, 5, u->s2, u->g2a, 2, s))) return e;
-    if ((e = conv_dgrad(u, 5, u->g2a, u->g2b, 2, s))) return e;                         // ds2 (skip to e2)
-    downsum_act_kernel<<<nblk(L[3].n * 2), 256, 0, s>>>(u->g2b, u->bb, u->g3a, L[3]);   // dz4
-    if ((e = conv_wgrad(u, 4, u->e3, u->g3a, 3, s))) return e;
-    if ((e = conv_dgrad(u, 4, u->g3a, u->g3b, 3, s))) return e;                         // de3
-    act_back_kernel<<<nblk(L[3].n * 2), 256, 0, s>>>(u->g3b, u->e3, u->g3a, L[3].n);    // dz3
-    if ((e = conv_wgrad(u, 3, u->p3, u->g3a, 3, s))) return e;
-    if ((e = conv_dgrad(u, 3, u->g3a, u->g3b, 3, s))) return e;                         // dp3
-    poolback_add_act_kernel<<<nblk(L[2].n * 2), 256, 0, s>>>(u->g2b, u->g3b, u->e2, u->g2a, L[2]);   // dz2
-    if ((e = conv_wgrad(u, 2, u->p2, u->g2a, 2, s))) return e;
-    if ((e = conv_dgrad(u, 2, u->g2a, u->g2c, 2, s))) return e;                         // dp2
-    poolback_add_act_kernel<<<nblk(L[1].n * 2), 256, 0, s>>>(u->g1b, u->g2c, u->e1, u->g1a, L[1]);   // dz1
-    if ((e = conv_wgrad(u, 1, u->p1, u->g1a, 1, s))) return e;
-    if ((e = conv_dgrad(u, 1, u->g1a, u->g1c, 1, s))) return e;                         // dp1
-    poolback_add_act_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->g0b, u->g1c, u->e0, u->g0a, L[0]);   // dz0
-    return conv_wgrad(u, 0, u->x0, u->g0a, 0, s);
+    // output conv (no activation), then the decoder from level 0 down
+    if ((e = conv_wgrad(u, NCONV - 1, u->d[0], u->ga[0], 0, s))) return e;
+    if ((e = conv_dgrad(u, NCONV - 1, u->ga[0], u->gc[0], 0, s))) return e;
+    act_back_kernel<<<nblk(L[0].n * 2), 256, 0, s>>>(u->gc[0], u->d[0], u->ga[0], L[0].n);   // dz of d0
+    for (int l = 0; l < NLEV; l++) {
+        const int c = 2 * NLEV - l;
+        if ((e = conv_wgrad(u, c, u->sm[l], u->ga[l], l, s))) return e;
+        if ((e = conv_dgrad(u, c, u->ga[l], u->gb[l], l, s))) return e;   // d(sum): skip part kept in gb
+        // through the upsample into the level below: d_{l+1}, or e_NLEV at the bottom
+        const __nv_bfloat16 *yb = (l + 1 < NLEV) ? u->d[l + 1] : u->e[NLEV];
+        downsum_act_kernel<<<nblk(L[l + 1].n * 2), 256, 0, s>>>(u->gb[l], yb, u->ga[l + 1], L[l + 1]);
+    }
+    // encoder from the bottom: ga[l] holds dz of e_l
+    for (int l = NLEV; l >= 1; l--) {
+        if ((e = conv_wgrad(u, l, u->p[l], u->ga[l], l, s))) return e;
+        if ((e = conv_dgrad(u, l, u->ga[l], u->gc[l], l, s))) return e;   // d(pooled input)
+        poolback_add_act_kernel<<<nblk(L[l - 1].n * 2), 256, 0, s>>>(u->gb[l - 1], u->gc[l], u->e[l - 1],
+                                                                       u->ga[l - 1], L[l - 1]);
+    }
+    return conv_wgrad(u, 0, u->x0, u->ga[0], 0, s);
 }
 
 // loss (relative squared error) of the current output against target t,
-// with its gradient into g0a; adds loss into scal[2]
+// with its gradient into ga[0]; adds loss into scal[2]
 cudaError_t loss_grad(UNetState *u, const float *t, double sumt2, cudaStream_t s)
 {
-    loss_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->out0, t, u->L[0].n, sumt2, u->g0a, u->scal + 2);
+    loss_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->out0, t, u->L[0].n, sumt2, u->ga[0], u->scal + 2);
     return cudaGetLastError();
 }
 
@@ -477,7 +475,8 @@ int unet_end_solve(UNetState *u, const GravArgs &a, bool converged, cudaStream_t
 }
 
 // `steps` Adam steps (learning rate decayed from lr to 0 on a cosine), each on
-// one stored sample (a seeded random order); mean loss of the last quarter
+// one stored sample (a seeded random order) under a random symmetry of the
+// box (48 for a cubic grid, 8 flips otherwise); mean loss of the last quarter
 int unet_train(UNetState *u, int steps, double lr, unsigned seed, double *mean_loss, cudaStream_t s)
 {
     if (steps < 0 || !(lr > 0.0)) return HC_ERR_ARG;
@@ -488,12 +487,21 @@ int unet_train(UNetState *u, int steps, double lr, unsigned seed, double *mean_l
     int nacc = 0;
     const int tail = std::max(1, steps / 4);
     cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
+    const Dims &d0 = u->L[0];
+    const bool cube = d0.nx == d0.ny && d0.ny == d0.nz;
+    static const int perms[6][3] = { { 0, 1, 2 }, { 0, 2, 1 }, { 1, 0, 2 }, { 1, 2, 0 }, { 2, 0, 1 }, { 2, 1, 0 } };
     for (int k = 0; k < steps; k++) {
         const int smp = (int)(rng() % (unsigned)u->count);
-        in_expand_kernel<<<nblk(n0 * 2), 256, 0, s>>>(u->sx + (size_t)smp * n0, n0, u->x0);
+        // a random symmetry of the (cubic) box: the map residual -> correction
+        // commutes with it, so the transformed pair is another valid sample
+        const int pi = cube ? (int)(rng() % 6u) : 0, flips = (int)(rng() % 8u);
+        const int sym = perms[pi][0] | (perms[pi][1] << 2) | (perms[pi][2] << 4) | (flips << 6);
+        symmetry_kernel<<<nblk(n0), 256, 0, s>>>(u->sx + (size_t)smp * n0, u->pooled, d0, sym);
+        symmetry_kernel<<<nblk(n0), 256, 0, s>>>(u->st + (size_t)smp * n0, u->xnorm, d0, sym);
+        in_expand_kernel<<<nblk(n0 * 2), 256, 0, s>>>(u->pooled, n0, u->x0);
         if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
         if (k == steps - tail) cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
-        if (loss_grad(u, u->st + (size_t)smp * n0, u->st2[smp], s) != cudaSuccess) return HC_ERR_CUDA;
+        if (loss_grad(u, u->xnorm, u->st2[smp], s) != cudaSuccess) return HC_ERR_CUDA;
         if (backward(u, s) != cudaSuccess) return HC_ERR_CUDA;
         // cosine decay of the learning rate over this call's steps
         const double lrk = lr * 0.5 * (1.0 + std::cos(3.14159265358979 * k / std::max(1, steps)));

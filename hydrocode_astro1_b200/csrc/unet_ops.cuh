@@ -345,6 +345,28 @@ __global__ void loss_kernel(const float *__restrict__ out0, const float *__restr
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, local * (sumt2 > 0.0 ? 1.0 / sumt2 : 0.0));
 }
 
+// One of the 48 symmetries of the cube applied to a level-0 volume: output
+// voxel (i0,i1,i2) reads input coordinate c[perm[a]] = flip[a] ? n-1-i_a : i_a
+// (perm and flips packed in `sym`: bits 0-1, 2-3, 4-5 = perm, bits 6-8 = flips).
+// Requires a cubic volume when perm is not the identity.
+__global__ void symmetry_kernel(const float *__restrict__ in, float *__restrict__ out, Dims d, int sym)
+{
+    const int p[3] = { sym & 3, (sym >> 2) & 3, (sym >> 4) & 3 };
+    const int n[3] = { d.nx, d.ny, d.nz };
+    UNET_LOOP(d.n)
+    {
+        int o[3];
+        voxel_ijk(d, t, o[0], o[1], o[2]);
+        int c[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const int v = ((sym >> (6 + a)) & 1) ? n[a] - 1 - o[a] : o[a];
+            c[p[a]] = v;
+        }
+        out[t] = in[vidx(d, c[0], c[1], c[2])];
+    }
+}
+
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
                             float *__restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2)
 {

@@ -177,11 +177,11 @@ int hc_sync(hc_ctx *ctx);
 int hc_timer_start(hc_ctx *ctx);
 int hc_timer_stop(hc_ctx *ctx, double *ms);
 
-/* Learned warm start (no reference counterpart).  A 3D U-Net (16 channels, 3
- * pooling levels, LeakyReLU, 49,377 parameters; BF16 weights and activations,
+/* Learned warm start (no reference counterpart).  A 3D U-Net (16 channels, 4
+ * pooling levels, LeakyReLU, 56,305 parameters; BF16 weights and activations,
  * FP32 accumulation on the tensor cores) maps the first FP64 residual of a
  * mixed-precision solve (HC_FP32, colour-split sweeps, grid dimensions
- * multiples of 16) to a correction of the previous potential:
+ * multiples of 32) to a correction of the previous potential:
  *   e0 = trilinear_up(net(pool2(delta) / rms)) * rms * kscale.
  * With warm_start = HC_WARM_UNET the solve starts from phi + e0 when that
  * lowers max|delta|, else from phi (counted in hc_diag); SOR then iterates to
@@ -196,7 +196,7 @@ int hc_timer_stop(hc_ctx *ctx, double *ms);
  * (lr, seeded sample order) of the relative squared error and returns the
  * mean loss of the last quarter of the steps.  hc_unet_loss_grad: one forward
  * and backward pass on host data at the network's level-0 dimensions (each a
- * multiple of 8; x normalised input, t target, nx*ny*nz values): loss, the
+ * multiple of 16; x normalised input, t target, nx*ny*nz values): loss, the
  * compact gradient and the output (each nullable). */
 int hc_unet_param_count(void);
 int hc_unet_init(hc_ctx *ctx, unsigned seed);

@@ -11,7 +11,8 @@ import numpy as np
 import torch
 import torch.nn.functional as F
 
-CH, NTAP, NCONV = 16, 27, 9
+CH, NTAP, NLEV = 16, 27, 4
+NCONV = 2 * NLEV + 2
 
 
 def unpack(params, dtype=torch.float64):
@@ -36,20 +37,19 @@ def unpack(params, dtype=torch.float64):
 
 
 def forward(layers, x):
-    """x: [nx, ny, nz] level-0 input -> output [nx, ny, nz]."""
+    """x: [nx, ny, nz] level-0 input -> output [nx, ny, nz].  Encoder convs
+    0..NLEV (pooling before each but the first), decoder convs NLEV+1..2 NLEV
+    on (nearest upsample + skip), output conv 2 NLEV + 1."""
     f = lambda z: F.leaky_relu(z, 0.1)
     conv = lambda h, l: F.conv3d(h, layers[l][0], layers[l][1], padding=1)
-    h0 = x[None, None]
-    e0 = f(conv(h0, 0))
-    e1 = f(conv(F.avg_pool3d(e0, 2), 1))
-    e2 = f(conv(F.avg_pool3d(e1, 2), 2))
-    e3 = f(conv(F.avg_pool3d(e2, 2), 3))
-    b = f(conv(e3, 4))
     up = lambda h: F.interpolate(h, scale_factor=2, mode="nearest")
-    d2 = f(conv(up(b) + e2, 5))
-    d1 = f(conv(up(d2) + e1, 6))
-    d0 = f(conv(up(d1) + e0, 7))
-    return conv(d0, 8)[0, 0]
+    e = [f(conv(x[None, None], 0))]
+    for l in range(1, NLEV + 1):
+        e.append(f(conv(F.avg_pool3d(e[-1], 2), l)))
+    h = e[NLEV]
+    for l in range(NLEV - 1, -1, -1):
+        h = f(conv(up(h) + e[l], 2 * NLEV - l))
+    return conv(h, NCONV - 1)[0, 0]
 
 
 def loss_and_grad(params, x, t, bf16_weights=True):

@@ -26,7 +26,7 @@ def smooth(shape, seed):
 
 
 def test_param_count():
-    assert hc.lib().hc_unet_param_count() == 49377
+    assert hc.lib().hc_unet_param_count() == 56305
 
 
 @pytest.mark.parametrize("seed", [3, 11])
@@ -35,8 +35,8 @@ def test_forward_and_gradient_match_oracle(seed):
     s.unet_init(seed)
     p, k = s.unet_params()
     assert k == 30.0
-    x = smooth((16, 16, 24), seed)
-    t = smooth((16, 16, 24), seed + 100) * 0.5
+    x = smooth((16, 16, 32), seed)
+    t = smooth((16, 16, 32), seed + 100) * 0.5
     lg, gg, og = s.unet_loss_grad(x, t)
     lr_, gr, orf = unet_ref.loss_and_grad(p, x, t)
     assert np.linalg.norm(og - orf) / np.linalg.norm(orf) < 2e-2
