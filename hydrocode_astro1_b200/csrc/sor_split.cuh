@@ -58,8 +58,8 @@ constexpr int SPLIT_BX = 32, SPLIT_BY = 8;
 // the z neighbour across a row end is a real cell of the adjacent row (rows
 // j-1 and j+1 exist for 1 <= j <= ny-2) and feeds only boundary cells, and a
 // CTA whose planes reach past nx-2 takes the guarded tail path.
-template <typename T, typename S, int NI>
-__global__ void __launch_bounds__(SPLIT_BX * SPLIT_BY)
+template <typename T, typename S, int NI, int MINB = 1>
+__global__ void __launch_bounds__(SPLIT_BX * SPLIT_BY, MINB)
 sor_split_kernel(T *__restrict__ own, const T *__restrict__ oth, const S *__restrict__ src, Split sp,
                  SorCoef<T> cf, int colour, double *res, int iter, double thresh, DevScalars *sc)
 {
@@ -189,12 +189,13 @@ template <typename T, typename S>
 cudaError_t launch_sor_split(T *base, const S *src, const Split &sp, const SorCoef<T> &cf, int colour,
                              double *res, int iter, double thresh, DevScalars *sc, cudaStream_t s)
 {
-    constexpr int NI = sizeof(T) == 8 ? 4 : 8;   // fastest at 256^3 (FP64 55.6, FP32 31.2 us per sweep)
+    constexpr int NI = sizeof(T) == 8 ? 4 : 8;   // fastest at 256^3: FP64 55.6, FP32 28.8 us per sweep
+    constexpr int MINB = sizeof(T) == 8 ? 1 : 4;
     if (sp.cs + 2LL * sp.ny * sp.H >= (1LL << 31)) return cudaErrorInvalidValue;   // 32-bit offsets
     dim3 grid((sp.H + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + NI - 1) / NI);
     T *own = base + (size_t)colour * sp.cs;
     const T *oth = base + (size_t)(colour ^ 1) * sp.cs;
-    sor_split_kernel<T, S, NI><<<grid, dim3(SPLIT_BX, SPLIT_BY), 0, s>>>(own, oth, src + (size_t)colour * sp.cs, sp,
+    sor_split_kernel<T, S, NI, MINB><<<grid, dim3(SPLIT_BX, SPLIT_BY), 0, s>>>(own, oth, src + (size_t)colour * sp.cs, sp,
                                                                          cf, colour, res, iter, thresh, sc);
     return cudaGetLastError();
 }

@@ -1,8 +1,12 @@
 // unet.cu -- the learned warm start: launchers of the tcgen05 convolution
 // kernels (unet_conv.cuh) and their C-ABI test hooks.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -15,9 +19,82 @@
 namespace hc {
 namespace unet {
 
+// 4D BF16 tensor map (c = 16, k, j, i) of a channels-last volume with a
+// {8, 10, 18, 1} box (one channel half of a halo plane), cached by pointer
+// and dimensions.  false if the driver entry point is missing or the layout
+// breaks a TMA rule.
+static bool halo_map(const __nv_bfloat16 *x, const Dims &d, CUtensorMap *out)
+{
+    static std::mutex mu;
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    struct Ent { const void *p; int nx, ny, nz; CUtensorMap m; };
+    static Ent cache[64];
+    static int used = 0, next = 0;
+    if ((uintptr_t)x % 16) return false;
+    std::lock_guard<std::mutex> lk(mu);
+    for (int t = 0; t < used; t++)
+        if (cache[t].p == x && cache[t].nx == d.nx && cache[t].ny == d.ny && cache[t].nz == d.nz) {
+            *out = cache[t].m;
+            return true;
+        }
+    if (!enc) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    cuuint64_t dims[4] = { (cuuint64_t)CH, (cuuint64_t)d.nz, (cuuint64_t)d.ny, (cuuint64_t)d.nx };
+    cuuint64_t strides[3] = { (cuuint64_t)CH * 2, (cuuint64_t)d.nz * CH * 2, (cuuint64_t)d.ny * d.nz * CH * 2 };
+    cuuint32_t box[4] = { 8, (cuuint32_t)HH_K, (cuuint32_t)HH_J, 1 };
+    cuuint32_t es[4] = { 1, 1, 1, 1 };
+    CUtensorMap m;
+    if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16 *>(x), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    cache[next] = Ent{ x, d.nx, d.ny, d.nz, m };
+    next = (next + 1) % 64;
+    if (used < 64) used++;
+    *out = m;
+    return true;
+}
+
+static bool halo_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("HC_NO_TMA");
+        on = (e && atoi(e) != 0) ? 0 : 1;
+    }
+    return on == 1;
+}
+
 cudaError_t conv3(const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *bias, void *out, const Dims &d,
                   int out_mode, int act, int *err, cudaStream_t s)
 {
+    CUtensorMap tm;
+    if (halo_enabled() && halo_map(x, d, &tm)) {
+        static int attr_dev = -1;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (attr_dev != dev) {
+            cudaError_t e = cudaFuncSetAttribute(conv3_halo_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)sizeof(HaloSmem));
+            if (e != cudaSuccess) return e;
+            attr_dev = dev;
+        }
+        const int tk = (d.nz + HT_K - 1) / HT_K, tj = (d.ny + HT_J - 1) / HT_J;
+        // about 6 CTAs per SM; at least 4 planes per CTA
+        const long long want = 148LL * 6;
+        int chunks = (int)std::max(1LL, std::min((long long)(d.nx + 3) / 4, (want + tk * tj - 1) / ((long long)tk * tj)));
+        const int chunk = (d.nx + chunks - 1) / chunks;
+        chunks = (d.nx + chunk - 1) / chunk;
+        conv3_halo_kernel<<<dim3(tk, tj, chunks), 128, sizeof(HaloSmem), s>>>(tm, w, bias, out, d, out_mode, act,
+                                                                              chunk, err);
+        return cudaGetLastError();
+    }
     const unsigned blocks = (unsigned)((d.n + TM - 1) / TM);
     conv3_kernel<<<blocks, 128, sizeof(ConvSmem), s>>>(x, w, bias, out, d, out_mode, act, err);
     return cudaGetLastError();

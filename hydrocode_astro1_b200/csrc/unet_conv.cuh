@@ -310,5 +310,168 @@ __global__ void wgrad_reduce_kernel(const float *__restrict__ partial, int npart
     dw[e] = s;
 }
 
+
+// ---------------------------------------------------------------------------
+// Halo-tile convolution (forward / input gradient) without an im2col copy.
+//
+// A CTA owns a 16 (j) x 8 (k) column of output voxels and marches along i.
+// Each input plane of the column plus its halo (18 x 10 voxels) is fetched by
+// two cp.async.bulk.tensor loads (one per 8-channel half, zero-filled outside
+// the volume) into a 4-slot ring laid out [half][j][k][8 ch]: 8 consecutive k
+// of one half are 128 contiguous bytes, i.e. one core matrix of a K-major
+// operand.  The A operand of tap (a,b,c) for output plane i is therefore a
+// descriptor into the halo of plane i+a-1 starting at row (b, c): SBO = 160
+// bytes (next j), LBO = one half-plane (2944-byte stride, channels 8..15).  Each
+// output plane is 27 MMAs (M=128 voxels, N=16, K=16 channels) accumulated in
+// one of two TMEM buffers; the epilogue of plane p-1 runs while the MMAs of
+// plane p execute, and the halo slot of plane p-2 is refilled once the MMAs
+// of plane p-1 have completed.
+// ---------------------------------------------------------------------------
+constexpr int HT_J = 16, HT_K = 8;                  // output tile
+constexpr int HH_J = HT_J + 2, HH_K = HT_K + 2;     // halo tile
+constexpr int HALF_BYTES = HH_J * HH_K * 16;        // 2880 loaded per channel half
+constexpr int HALF_STRIDE = 2944;                   // 128-byte aligned stride (the descriptor LBO)
+constexpr int SLOT_BYTES = 2 * HALF_STRIDE;         // 5888
+constexpr int NSLOT = 4;
+
+struct HaloSmem {
+    __align__(128) unsigned char slot[NSLOT][SLOT_BYTES];
+    __align__(128) unsigned char w[NTAP][512];      // B per tap: 16 co x 16 ci, K-major
+    __align__(8) uint64_t tbar[NSLOT];
+    __align__(8) uint64_t mbar[2];
+    uint32_t tmem;
+};
+
+__device__ __forceinline__ void halo_load(const CUtensorMap *tm, HaloSmem &sm, int slot, int k0, int j0, int i)
+{
+    uint64_t *bar = &sm.tbar[slot];
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)),
+                 "r"((unsigned)(2 * HALF_BYTES))
+                 : "memory");
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                     " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(tc::smem_u32(sm.slot[slot] + h * HALF_STRIDE)),
+                     "l"(reinterpret_cast<uint64_t>(tm)), "r"(8 * h), "r"(k0 - 1), "r"(j0 - 1), "r"(i),
+                     "r"(tc::smem_u32(bar))
+                     : "memory");
+}
+
+__global__ void __launch_bounds__(128)
+conv3_halo_kernel(const __grid_constant__ CUtensorMap tmx, const __nv_bfloat16 *__restrict__ w,
+                  const float *__restrict__ bias, void *__restrict__ out, Dims d, int out_mode, int act, int chunk,
+                  int *err)
+{
+    extern __shared__ __align__(128) unsigned char smraw[];
+    HaloSmem &sm = *reinterpret_cast<HaloSmem *>(smraw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k0 = blockIdx.x * HT_K, j0 = blockIdx.y * HT_J;
+    const int i0 = blockIdx.z * chunk, i1 = min(d.nx, i0 + chunk);
+    if (i0 >= i1) return;
+    const int np = i1 - i0;
+
+    if (warp == 0) {
+        tc::tmem_alloc(&sm.tmem, 32);
+        tc::fence_before();
+    }
+    if (tid == 0) {
+        for (int q = 0; q < NSLOT; q++) tc::bar_init(&sm.tbar[q], 1);
+        tc::bar_init(&sm.mbar[0], 1);
+        tc::bar_init(&sm.mbar[1], 1);
+    }
+    // weights: B of tap t, row co, K = ci: (co/8)*256 + (ci/8)*128 + (co%8)*16 + (ci%8)*2
+    for (int q = tid; q < NTAP * CH * 2; q += blockDim.x) {
+        const int tap = q / (CH * 2), rem = q % (CH * 2), co = rem >> 1, half = rem & 1;
+        const uint4 v = *reinterpret_cast<const uint4 *>(w + ((size_t)co * NTAP + tap) * CH + half * 8);
+        *reinterpret_cast<uint4 *>(sm.w[tap] + (co >> 3) * 256 + half * 128 + (co & 7) * 16) = v;
+    }
+    tc::fence_smem_to_async();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = sm.tmem;
+    constexpr uint32_t IDESC = tc::idesc_bf16(TM, CH);
+    bool ok = true;
+    unsigned tph[NSLOT] = { 0, 0, 0, 0 }, mph[2] = { 0, 0 };
+    auto slot_of = [](int plane) { return (plane + 4) & 3; };   // plane >= -1
+
+    if (tid == 0) {
+        halo_load(&tmx, sm, slot_of(i0 - 1), k0, j0, i0 - 1);
+        halo_load(&tmx, sm, slot_of(i0), k0, j0, i0);
+        halo_load(&tmx, sm, slot_of(i0 + 1), k0, j0, i0 + 1);
+    }
+    auto wait_plane = [&](int plane) {
+        const int sl = slot_of(plane);
+        ok = tc::bar_wait(&sm.tbar[sl], tph[sl] & 1) && ok;
+        tph[sl]++;
+    };
+    auto epilogue = [&](int p) {
+        const int b = p & 1;
+        ok = tc::bar_wait(&sm.mbar[b], mph[b] & 1) && ok;
+        mph[b]++;
+        tc::fence_after();
+        float acc[16];
+        tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + b * 16, acc);
+        const int r = warp * 32 + lane, jj = r >> 3, kk = r & 7;
+        const int j = j0 + jj, k = k0 + kk, i = i0 + p;
+        if (j < d.ny && k < d.nz) {
+            const long long vo = ((long long)i * d.ny + j) * d.nz + k;
+            if (out_mode == 2) {
+                reinterpret_cast<float *>(out)[vo] = acc[0] + bias[0];
+            } else if (out_mode == 3) {
+                float *o = reinterpret_cast<float *>(out) + vo * CH;
+#pragma unroll
+                for (int t = 0; t < 16; t++) o[t] = acc[t] + bias[t];
+            } else {
+                __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+                for (int t = 0; t < 16; t++) {
+                    float y = acc[t];
+                    if (out_mode == 0) {
+                        y += bias[t];
+                        if (act) y = leaky(y);
+                    }
+                    h[t] = __float2bfloat16(y);
+                }
+                uint4 *o = reinterpret_cast<uint4 *>(reinterpret_cast<__nv_bfloat16 *>(out) + vo * CH);
+                o[0] = *reinterpret_cast<const uint4 *>(&h[0]);
+                o[1] = *reinterpret_cast<const uint4 *>(&h[8]);
+            }
+        }
+    };
+
+    wait_plane(i0 - 1);
+    wait_plane(i0);
+    for (int p = 0; p < np; p++) {
+        const int i = i0 + p;
+        wait_plane(i + 1);
+        if (tid == 0) {
+            tc::fence_after();
+            const uint32_t wb = tc::smem_u32(sm.w[0]);
+#pragma unroll 1
+            for (int a = 0; a < 3; a++) {
+                const uint32_t base = tc::smem_u32(sm.slot[slot_of(i + a - 1)]);
+#pragma unroll
+                for (int bc = 0; bc < 9; bc++) {
+                    const int b = bc / 3, c = bc % 3, tap = a * 9 + bc;
+                    const uint64_t da = tc::sdesc(base + (b * HH_K + c) * 16, HALF_STRIDE, HH_K * 16);
+                    const uint64_t db = tc::sdesc(wb + tap * 512, 128, 256);
+                    tc::mma_bf16(tmem + (p & 1) * 16, da, db, IDESC, tap > 0 ? 1u : 0u);
+                }
+            }
+            tc::mma_commit(&sm.mbar[p & 1]);
+        }
+        if (p >= 1) epilogue(p - 1);   // also: the MMAs of plane p-1 are done
+        if (tid == 0 && p + 2 < np + 1) halo_load(&tmx, sm, slot_of(i + 2), k0, j0, i + 2);
+        tc::fence_before();
+        __syncthreads();   // TMEM buffer of plane p-1 read by all before plane p+1 reuses it
+    }
+    epilogue(np - 1);
+    // the last halo load (plane i1) was consumed by the last plane; planes past it were not issued
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 32);
+    if (!ok && tid == 0) atomicExch(err, -6);
+}
+
 }  // namespace unet
 }  // namespace hc
