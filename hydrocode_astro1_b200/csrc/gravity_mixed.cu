@@ -332,45 +332,55 @@ __device__ __forceinline__ double block_max_any(double v)
 }
 
 // r32 / e32 in the natural layout, or colour-split (sp.cs > 0)
+// One (i, j) row per block iteration, threads along k (no per-cell index
+// division).  r32 / e32 in the natural layout, or colour-split (sp.cs > 0).
 __global__ void __launch_bounds__(256) mixed_residual_kernel(GravArgs a, float *r32, float *e32, Split sp)
 {
     const Geom g = a.g;
     const MixConst mc = mix_const(a);
+    const double ifac = 1.0 / mc.fac;
     const long long sI = (long long)g.ny * g.nz, sJ = g.nz;
+    const long long rows = (long long)g.nx * g.ny;
     double m = 0.0;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.n;
-         c += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(c / sI), j = (int)((c / sJ) % g.ny), k = (int)(c % sJ);
-        const long long o = sp.cs ? sp.at(i, j, k) : c;
-        float d = 0.f;
-        if (i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2 && k >= 1 && k <= g.nz - 2) {
-            const double *phi = a.phi;
-            double lap = (phi[c - sI] + phi[c + sI]) * mc.ix2 + (phi[c - sJ] + phi[c + sJ]) * mc.iy2 +
-                         (phi[c - 1] + phi[c + 1]) * mc.iz2;
-            double rr = a.rho ? a.rho[c] : (double)a.rho32[c];
-            double dd = (lap - mc.fpg * rr) / mc.fac - phi[c];
-            m = tmax(m, fabs(dd));
-            d = (float)dd;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int i = (int)(row / g.ny), j = (int)(row % g.ny);
+        const bool inner = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
+        const long long c0 = row * sJ;
+        for (int k = threadIdx.x; k < g.nz; k += blockDim.x) {
+            const long long c = c0 + k;
+            const long long o = sp.cs ? sp.at(i, j, k) : c;
+            float d = 0.f;
+            if (inner && k >= 1 && k <= g.nz - 2) {
+                const double *phi = a.phi;
+                const double lap = (phi[c - sI] + phi[c + sI]) * mc.ix2 + (phi[c - sJ] + phi[c + sJ]) * mc.iy2 +
+                                   (phi[c - 1] + phi[c + 1]) * mc.iz2;
+                const double rr = a.rho ? a.rho[c] : (double)a.rho32[c];
+                const double dd = (lap - mc.fpg * rr) * ifac - phi[c];
+                m = tmax(m, fabs(dd));
+                d = (float)dd;
+            }
+            r32[o] = d;
+            e32[o] = 0.f;
         }
-        r32[o] = d;
-        e32[o] = 0.f;
     }
     double b = block_max_any<256>(m);
     if (threadIdx.x == 0) atomic_max_nonneg((unsigned long long *)&a.sc->resnorm, b);
 }
 
-// phi += e; max|e| into sc->resid_bits (the FP32 resolution check)
+// phi += sign * e; max|e| into sc->resid_bits (the FP32 resolution check)
 __global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const float *e32, Split sp, float sign)
 {
-    const long long sI = (long long)a.g.ny * a.g.nz, sJ = a.g.nz;
+    const long long rows = (long long)a.g.nx * a.g.ny;
     float m = 0.f;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < a.g.n;
-         c += (long long)gridDim.x * blockDim.x) {
-        long long o = c;
-        if (sp.cs) o = sp.at((int)(c / sI), (int)((c / sJ) % a.g.ny), (int)(c % sJ));
-        const float e = sign * e32[o];
-        a.phi[c] += (double)e;
-        m = tmax(m, fabsf(e));
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int i = (int)(row / a.g.ny), j = (int)(row % a.g.ny);
+        const long long c0 = row * a.g.nz;
+        for (int k = threadIdx.x; k < a.g.nz; k += blockDim.x) {
+            const long long o = sp.cs ? sp.at(i, j, k) : c0 + k;
+            const float e = sign * e32[o];
+            a.phi[c0 + k] += (double)e;
+            m = tmax(m, fabsf(e));
+        }
     }
     const double b = block_max_any<256>((double)m);
     if (threadIdx.x == 0 && b > 0.0) atomic_max_nonneg(&a.sc->resid_bits, b);
@@ -429,13 +439,13 @@ static Split split_or_natural(const GravArgs &a, bool split)
 
 cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, bool split, cudaStream_t s)
 {
-    mixed_residual_kernel<<<148 * 8, 256, 0, s>>>(a, r32, e32, split_or_natural(a, split));
+    mixed_residual_kernel<<<148 * 16, 256, 0, s>>>(a, r32, e32, split_or_natural(a, split));
     return cudaGetLastError();
 }
 
 cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, float sign, cudaStream_t s)
 {
-    mixed_update_kernel<<<148 * 8, 256, 0, s>>>(a, e32, split_or_natural(a, split), sign);
+    mixed_update_kernel<<<148 * 16, 256, 0, s>>>(a, e32, split_or_natural(a, split), sign);
     return cudaGetLastError();
 }
 

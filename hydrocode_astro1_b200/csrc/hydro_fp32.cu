@@ -91,9 +91,9 @@ cudaError_t fp32_interior(const HydroArgs &a, int chunks, cudaStream_t s)
         CUtensorMap tm;
         cudaError_t e = encode_state_map(a, &tm);
         if (e == cudaSuccess) {
-            // 3 CTAs per SM, about 4 waves
+            // 4 CTAs per SM, about 4 waves
             long long tiles = (long long)((a.g.nz + tma32::TK - 1) / tma32::TK) * ((a.g.ny + tma32::TJ - 1) / tma32::TJ);
-            long long want = 148LL * 3 * 4;
+            long long want = 148LL * 4 * 4;
             int nint = a.g.nx - 2;
             int ch = (int)std::max(1LL, std::min((want + tiles - 1) / tiles, (long long)std::max(1, nint / 8)));
             int ilen = (nint + ch - 1) / ch;

@@ -141,7 +141,7 @@ __device__ __forceinline__ void tma_plane(const CUtensorMap *tm, float *dst, uin
                  : "memory");
 }
 
-__global__ void __launch_bounds__(NT, 3)
+__global__ void __launch_bounds__(NT, 4)
 interior_tma_kernel(const __grid_constant__ CUtensorMap tmap, HydroArgs a, int ilen)
 {
     __shared__ __align__(128) float raw[2][RAWP];
