@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--unet-passes", type=int, default=1, help="learned-start predictions per solve")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="skip the FP32 arm without the learned warm start")
     return ap.parse_args()
@@ -163,6 +164,7 @@ def solver_kwargs(p, variant, device):
 # `python -m hydrocode_astro1_b200.train_unet` from solves of this workload
 # with another density-noise seed (7); the benchmark run uses seed 42.
 UNET_WEIGHTS = os.path.join(ROOT, "hydrocode_astro1_b200", "data", "unet_stellar_explosion_256.bin")
+UNET_PASSES = 1
 
 
 def make_solver(p, variant, device):
@@ -170,6 +172,7 @@ def make_solver(p, variant, device):
     s = hc.HydroSolver3D(p["shape"], **solver_kwargs(p, variant, device))
     if variant == "fp32_unet":
         s.unet_load_file(UNET_WEIGHTS)
+        s.unet_passes(UNET_PASSES)
     return s
 
 
@@ -340,6 +343,9 @@ def main_reference(args):
 # ---------------------------------------------------------------- our arm
 def main_ours(args):
     import numpy as np
+
+    global UNET_PASSES
+    UNET_PASSES = args.unet_passes
 
     import hydrocode_astro1_b200 as hc
     world, rank, local, dist = dist_setup(args)

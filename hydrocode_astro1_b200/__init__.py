@@ -104,6 +104,7 @@ CAPI = {
     "hc_unet_save_file": (C.c_int, [C.c_void_p, C.c_char_p]),
     "hc_unet_collect": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_unet_samples": (C.c_int, [C.c_void_p]),
+    "hc_set_unet_passes": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_unet_train": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint, C.POINTER(C.c_double)]),
     "hc_unet_loss_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float),
@@ -340,6 +341,9 @@ class HydroSolver3D:
 
     def unet_samples(self):
         return self.L.hc_unet_samples(self.h)
+
+    def unet_passes(self, n):
+        _check(self.L.hc_set_unet_passes(self.h, int(n)), "hc_set_unet_passes")
 
     def unet_train(self, steps, lr=1e-3, seed=0):
         loss = C.c_double(0.0)

@@ -99,6 +99,7 @@ struct hc_ctx {
     cudaEvent_t t0, t1;
     int timer_on;
     int debug;                   // HC_DEBUG=1: per-solve progress on stderr
+    int unet_passes;             // learned-start predictions per solve (>= 1)
 };
 
 static cudaEvent_t ev_get(hc_ctx *c)
@@ -692,29 +693,41 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
             if (predict || unet_collecting(c->unet)) {
                 {
                     FamTimer t(c, FAM_UNET);
-                    rc = unet_begin_solve(c->unet, a, c->r32, predict ? c->e32b : nullptr, c->s);
+                    rc = unet_begin_solve(c->unet, a, c->r32, predict ? c->e32b : nullptr, true, c->s);
                     c->launches += predict ? 40 : 3;
                 }
                 if (rc) return set_err(rc, "learned warm start: grid dimensions must be multiples of 32");
                 recorded = unet_collecting(c->unet);
             }
-            if (predict) {
+            // passes after the first predict from the residual the previous
+            // accepted pass left, until one is rejected
+            for (int pass = 0; predict && pass < std::max(1, c->unet_passes); pass++) {
+                if (pass > 0) {
+                    FamTimer t(c, FAM_UNET);
+                    rc = unet_begin_solve(c->unet, a, c->r32, c->e32b, false, c->s);
+                    if (rc) return set_err(rc, "learned warm start failed");
+                    c->launches += 40;
+                }
                 CK(mixed_update(a, c->e32b, split, 1.0f, c->s));
                 double d1 = 0.0;
                 rc = residual(&d1);
                 if (rc) return rc;
-                if (c->debug) fprintf(stderr, "[hc] learned start: max|delta| %.3e -> %.3e\n", dmax, d1);
+                c->launches += 2;
+                if (c->debug) fprintf(stderr, "[hc] learned start %d: max|delta| %.3e -> %.3e\n", pass, dmax, d1);
                 if (std::isfinite(d1) && d1 < dmax) {
                     dmax = d1;
-                    c->diag.warm_start_used = 1;
-                    c->diag.unet_accepted++;
-                } else {
-                    CK(mixed_update(a, c->e32b, split, -1.0f, c->s));
-                    rc = residual(&dmax);
-                    if (rc) return rc;
-                    c->diag.unet_fallbacks++;
+                    if (pass == 0) {
+                        c->diag.warm_start_used = 1;
+                        c->diag.unet_accepted++;
+                    }
+                    continue;
                 }
+                CK(mixed_update(a, c->e32b, split, -1.0f, c->s));
+                rc = residual(&dmax);
+                if (rc) return rc;
                 c->launches += 2;
+                if (pass == 0) c->diag.unet_fallbacks++;
+                break;
             }
         }
         if (c->debug) fprintf(stderr, "[hc] mixed cycle %d: max|delta| %.3e after %d sweeps\n", cycles, dmax, total);
@@ -1327,4 +1340,11 @@ extern "C" int hc_unet_loss_grad(hc_ctx *c, int nx, int ny, int nz, const float 
     CK(cudaSetDevice(c->dev));
     const int rc = unet_loss_grad(c->unet, nx, ny, nz, x, t, loss, grad, out, c->s);
     return rc ? set_err(rc, "U-Net loss/gradient failed") : HC_OK;
+}
+
+extern "C" int hc_set_unet_passes(hc_ctx *c, int passes)
+{
+    if (!c || passes < 1 || passes > 8) return set_err(HC_ERR_ARG, "passes must be 1..8");
+    c->unet_passes = passes;
+    return HC_OK;
 }

@@ -194,7 +194,7 @@ int unet_init(UNetState *u, unsigned seed, cudaStream_t s);
 int unet_collect(UNetState *u, int capacity);
 int unet_samples(const UNetState *u);
 bool unet_collecting(const UNetState *u);
-int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e_out, cudaStream_t s);
+int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e_out, bool record, cudaStream_t s);
 int unet_end_solve(UNetState *u, const GravArgs &a, bool converged, cudaStream_t s);
 int unet_train(UNetState *u, int steps, double lr, unsigned seed, double *mean_loss, cudaStream_t s);
 int unet_loss_grad(UNetState *u, int n0x, int n0y, int n0z, const float *x, const float *t, double *loss, float *grad,

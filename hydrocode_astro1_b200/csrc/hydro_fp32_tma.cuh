@@ -198,6 +198,23 @@ interior_tma_kernel(const __grid_constant__ CUtensorMap tmap, HydroArgs a, int i
             P[s] = rec_at(r, sj, sk + 3);
         }
     };
+    // the NH = 2 SK + 2 TJ records around the tile: rows 0 and SJ-1, then the
+    // first and last column of rows 1..TJ
+    constexpr int NH = 2 * SK + 2 * TJ;
+    auto build_halo = [&](const float *r) {
+        if (tid < NH) {
+            int sj, sk;
+            if (tid < 2 * SK) {
+                sj = (tid < SK) ? 0 : SJ - 1;
+                sk = tid % SK;
+            } else {
+                const int q = tid - 2 * SK;
+                sj = 1 + (q >> 1);
+                sk = (q & 1) ? SK - 1 : 0;
+            }
+            P[sj * SK + sk] = rec_at(r, sj, sk + 3);
+        }
+    };
 
     issue(ib - 1);
     issue(ib);
@@ -228,7 +245,10 @@ interior_tma_kernel(const __grid_constant__ CUtensorMap tmap, HydroArgs a, int i
             }
         }
         __syncthreads();
-        build_P(rn);        // plane i+1 for the next iteration
+        // plane i+1 for the next iteration: this thread's own record is nx1;
+        // threads 0..NH-1 form the halo ring's records
+        P[(ty + 1) * SK + tx + 1] = nx1;
+        build_halo(rn);
         if (own_int && k < nz && j < ny) {
             const Flux &yp = FY[(ty + 1) * TK + tx], &ym = FY[ty * TK + tx];
             const Flux &zp = FZ[ty * (TK + 1) + tx + 1], &zm = FZ[ty * (TK + 1) + tx];

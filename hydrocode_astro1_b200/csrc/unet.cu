@@ -504,14 +504,14 @@ bool unet_collecting(const UNetState *u) { return u && u->cap > 0; }
 // (r32, colour split): prepare the network input and, when `e_out` is given,
 // predict the correction into it (colour split, zero on boundary cells).
 // When collecting, also record the input and a copy of phi for the target.
-int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e_out, cudaStream_t s)
+int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e_out, bool record, cudaStream_t s)
 {
     int rc = ensure_grid(u, a.g.nx, a.g.ny, a.g.nz);
     if (rc) return rc;
     const Split sp = make_split(a.g);
     cudaMemsetAsync(u->scal, 0, sizeof(double), s);
     in_pool_kernel<<<nblk(u->L[0].n), 256, 0, s>>>(r32, sp, u->L[0], u->pooled, u->scal);
-    const bool collect = u->cap > 0 && u->sx;
+    const bool collect = record && u->cap > 0 && u->sx;
     u->slot = collect ? u->next : -1;
     float *xs = collect ? u->sx + (size_t)u->slot * u->L[0].n : nullptr;
     in_norm_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->pooled, u->scal, u->L[0].n, u->x0, xs);

@@ -209,6 +209,9 @@ int hc_unet_samples(hc_ctx *ctx);
 int hc_unet_train(hc_ctx *ctx, int steps, double lr, unsigned seed, double *mean_loss);
 int hc_unet_loss_grad(hc_ctx *ctx, int nx, int ny, int nz, const float *x, const float *t, double *loss,
                       float *grad, float *out);
+/* Predictions per solve (1..8, default 1): after an accepted prediction the
+ * network is applied again to the residual it left, until one is rejected. */
+int hc_set_unet_passes(hc_ctx *ctx, int passes);
 
 /* Diagnostics of the tensor-core convolution kernels (no reference
  * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16
