@@ -100,6 +100,7 @@ struct hc_ctx {
     int timer_on;
     int debug;                   // HC_DEBUG=1: per-solve progress on stderr
     int unet_passes;             // learned-start predictions per solve (>= 1)
+    int unet_cycles;             // correction cycles that start from a prediction (0: 2)
 };
 
 static cudaEvent_t ev_get(hc_ctx *c)
@@ -306,7 +307,9 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
         rc = dmalloc((void **)&c->phi, n * sizeof(double));
         if (!rc) rc = dmalloc((void **)&c->phig, n * sizeof(double));
         if (!rc) rc = ensure_res(c, k.max_iter);
-        c->scratch_len = 64 * 1024;   // tree partials (592x9) and lmax partials (296x169)
+        // tree partials (592x9), lmax partials (<= 387x169), then the lmax
+        // z-power sums (13 per (i, j) row)
+        c->scratch_len = 64 * 1024 + (long long)c->g.nx * c->g.ny * 13;
         if (!rc) rc = dmalloc((void **)&c->scratch, c->scratch_len * sizeof(double));
         if (!rc) rc = dmalloc((void **)&c->mom, 4 * 1024 * sizeof(double));
         if (!rc && k.precision == HC_FP32) {
@@ -684,20 +687,27 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         rc = residual(&dmax);
         if (rc) return rc;
         cycles++;
-        // Learned warm start (first cycle, colour-split layout): the network
-        // predicts the correction from this residual; phi + e0 is kept only
-        // if its FP64 residual is smaller, else phi is restored.  With sample
-        // collection on, the residual and phi are recorded for training.
-        if (cycles == 1 && split && c->unet && std::isfinite(dmax)) {
+        // Learned warm start (the first unet_cycles correction cycles,
+        // colour-split layout): the network predicts the correction from this
+        // residual; phi + e0 is kept only if its FP64 residual is smaller, else
+        // phi is restored.  The first cycle's residual is the step's (rough,
+        // after the hydro update); the second's is what the first cycle's
+        // sweeps left (smooth), where the prediction removes the slow modes
+        // that the remaining sweeps would spend most of their iterations on.
+        // With sample collection on, the first cycle's residual and phi are
+        // recorded for training.
+        const int ucycles = c->unet_cycles > 0 ? c->unet_cycles : 2;
+        if (cycles <= ucycles && split && c->unet && std::isfinite(dmax)) {
             const bool predict = c->cfg.warm_start == HC_WARM_UNET && unet_has_weights(c->unet);
-            if (predict || unet_collecting(c->unet)) {
+            const bool rec = cycles == 1 && unet_collecting(c->unet);
+            if (predict || rec) {
                 {
                     FamTimer t(c, FAM_UNET);
-                    rc = unet_begin_solve(c->unet, a, c->r32, predict ? c->e32b : nullptr, true, c->s);
+                    rc = unet_begin_solve(c->unet, a, c->r32, predict ? c->e32b : nullptr, rec, c->s);
                     c->launches += predict ? 40 : 3;
                 }
                 if (rc) return set_err(rc, "learned warm start: grid dimensions must be multiples of 32");
-                recorded = unet_collecting(c->unet);
+                if (rec) recorded = true;
             }
             // passes after the first predict from the residual the previous
             // accepted pass left, until one is rejected
@@ -716,7 +726,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
                 if (c->debug) fprintf(stderr, "[hc] learned start %d: max|delta| %.3e -> %.3e\n", pass, dmax, d1);
                 if (std::isfinite(d1) && d1 < dmax) {
                     dmax = d1;
-                    if (pass == 0) {
+                    if (pass == 0 && cycles == 1) {
                         c->diag.warm_start_used = 1;
                         c->diag.unet_accepted++;
                     }
@@ -726,7 +736,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
                 rc = residual(&dmax);
                 if (rc) return rc;
                 c->launches += 2;
-                if (pass == 0) c->diag.unet_fallbacks++;
+                if (pass == 0 && cycles == 1) c->diag.unet_fallbacks++;
                 break;
             }
         }
@@ -1346,5 +1356,12 @@ extern "C" int hc_set_unet_passes(hc_ctx *c, int passes)
 {
     if (!c || passes < 1 || passes > 8) return set_err(HC_ERR_ARG, "passes must be 1..8");
     c->unet_passes = passes;
+    return HC_OK;
+}
+
+extern "C" int hc_set_unet_cycles(hc_ctx *c, int cycles)
+{
+    if (!c || cycles < 1 || cycles > 8) return set_err(HC_ERR_ARG, "cycles must be 1..8");
+    c->unet_cycles = cycles;
     return HC_OK;
 }

@@ -9,8 +9,8 @@
 // centre of mass is
 //   phi(r) = -G sum_l sum_m N_lm (C_lm Re Q_l^m(r) + S_lm Im Q_l^m(r)) / r^(2l+1)
 // with C_lm + i S_lm = sum_cells rho dV N_lm Q_l^m(r').  Coefficients are stored
-// at l*l+l+m (C, m >= 0) and l*l+l-m (S, m > 0).  The sums are FP64 and use a
-// fixed-shape tree, so they are deterministic.
+// at l*l+l+m (C, m >= 0) and l*l+l-m (S, m > 0).  The sums are FP64 in a
+// fixed order (rows, then blocks), so they are deterministic.
 #include <algorithm>
 
 #include "hc_internal.cuh"
@@ -25,6 +25,7 @@ namespace {
 
 constexpr int LM_MAX = 12;
 constexpr int LM_NC = (LM_MAX + 1) * (LM_MAX + 1);
+constexpr long long LM_SCRATCH0 = 64 * 1024;   // doubles of partial sums before the z-power sums
 
 __constant__ double c_norm[LM_NC];   // N_lm at l*(LM_MAX+1)+m
 
@@ -62,40 +63,173 @@ __device__ __forceinline__ void solid_harmonics(double x, double y, double z, in
     }
 }
 
-__constant__ double c_rinv[LM_MAX + 1];   // 1 / d for d = l - m >= 2 (index d)
+// Row-factored moments.  For a fixed order m, Q_l^m = Q_m^m(x, y) p_l^m(z),
+// where Q_m^m depends only on (x, y) -- constant along a row (i, j) -- and
+// p_l^m is a real polynomial in z of degree l - m whose coefficients follow
+// from the recursion with r^2 = rho2 + z^2, rho2 = x^2 + y^2:
+//   p_m = 1,  p_{m+1} = (2m+1) z,
+//   (l-m) p_l = (2l-1) z p_{l-1} - (l+m-1) (rho2 + z^2) p_{l-2}.
+// Hence sum_k rho_k Q_l^m(x, y, z_k) = Q_m^m(x, y) sum_t c_lt Z_t, with the
+// row's z-power sums Z_t = sum_k rho_k z_k^t (t <= lmax).  One pass over the
+// density forms Z_t for every row (HBM-bound); a second, per (row, m), runs
+// the coefficient recursion and accumulates the row's contribution.  The
+// centre of mass comes first from the row sums of rho and rho z.
+constexpr int LR_NT = 256;           // 8 warps; one row per warp at a time
+constexpr int LR_ROWBLK = 128;       // rows per block of lmax_rows
+constexpr int LR_UNROLL = 8;         // density loads in flight per lane
 
-// Solid-harmonic moments, one order m per warp: block b takes the (i,j) rows
-// b, b + gridDim, ..., lane L the cells k = L, L+32, ... of each row, and
-// accumulates, in registers, dm N_lm Q_l^m
-// for l = m..lmax with the recursion of solid_harmonics (same operations, the
-// division by l-m replaced by the identical product with 1/(l-m) computed on
-// the host); a fixed butterfly reduction per warp writes this block's partial
-// sums, which lmax_final adds in block order.
-template <int LMAX>
-__global__ void __launch_bounds__(32 * (LMAX + 1)) lmax_partial(GravArgs a, const double *com)
+__device__ __forceinline__ double dens(const GravArgs &a, long long c)
+{
+    return a.rho ? a.rho[c] : (double)a.rho32[c];
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Centre of mass, partial sums per CTA: (S0, x S0, y S0, S1) over its rows,
+// S0 = sum_k rho, S1 = sum_k rho z (cells with rho > 0, as in every moment).
+__global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a)
 {
     const Geom g = a.g;
-    constexpr int lmax = LMAX;
-    const int m = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (m > lmax) return;
-    const double dV = g.dx * g.dy * g.dz;
-    const long long snz = g.nz;
-    const double xc = com[0], yc = com[1], zc = com[2];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long rows = (long long)g.nx * g.ny;
+    double v0 = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+    for (long long row = (long long)blockIdx.x * (LR_NT / 32) + warp; row < rows;
+         row += (long long)gridDim.x * (LR_NT / 32)) {
+        const long long base = row * g.nz;
+        double s0 = 0.0, s1 = 0.0;
+        for (int k0 = 0; k0 < g.nz; k0 += 32 * LR_UNROLL) {
+            double rv[LR_UNROLL];
+#pragma unroll
+            for (int u = 0; u < LR_UNROLL; u++) {
+                const int k = k0 + 32 * u + lane;
+                rv[u] = k < g.nz ? dens(a, base + k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < LR_UNROLL; u++) {
+                if (rv[u] > 0.0) {
+                    s0 += rv[u];
+                    s1 += rv[u] * (g.zmin + (k0 + 32 * u + lane + 0.5) * g.dz);
+                }
+            }
+        }
+        s0 = warp_sum(s0);
+        s1 = warp_sum(s1);
+        const int i = (int)(row / g.ny), j = (int)(row % g.ny);
+        v0 += s0;
+        vx += (g.xmin + (i + 0.5) * g.dx) * s0;
+        vy += (g.ymin + (j + 0.5) * g.dy) * s0;
+        vz += s1;
+    }
+    __shared__ double red[LR_NT / 32][4];
+    if (lane == 0) {
+        red[warp][0] = v0;
+        red[warp][1] = vx;
+        red[warp][2] = vy;
+        red[warp][3] = vz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double s = 0.0;
+        for (int w = 0; w < LR_NT / 32; w++) s += red[w][threadIdx.x];
+        a.scratch[(long long)blockIdx.x * 4 + threadIdx.x] = s;
+    }
+}
+
+// M = dV S0 and the centre of mass (box centre when there is no mass), as
+// the reference's monopole pass stores them
+__global__ void lmax_com_final(GravArgs a, int nparts)
+{
+    __shared__ double v[4];
+    const int q = threadIdx.x;
+    if (q < 4) {
+        double s = 0.0;
+        for (int b = 0; b < nparts; b++) s += a.scratch[(long long)b * 4 + q];
+        v[q] = s;
+    }
+    __syncthreads();
+    if (q != 0) return;
+    const Geom g = a.g;
+    a.sc->moments[0] = v[0] * (g.dx * g.dy * g.dz);
+    if (v[0] > 0.0) {
+        a.sc->moments[1] = v[1] / v[0];
+        a.sc->moments[2] = v[2] / v[0];
+        a.sc->moments[3] = v[3] / v[0];
+    } else {
+        a.sc->moments[1] = 0.5 * (g.xmin + g.xmax);
+        a.sc->moments[2] = 0.5 * (g.ymin + g.ymax);
+        a.sc->moments[3] = 0.5 * (g.zmin + g.zmax);
+    }
+}
+
+// z-power sums about the centre of mass: zs[t * rows + row] = sum_k rho z^t
+template <int LMAX>
+__global__ void __launch_bounds__(LR_NT) lmax_zsums(GravArgs a, const double *com, double *zs)
+{
+    const Geom g = a.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long rows = (long long)g.nx * g.ny;
+    const double z0 = g.zmin - com[2];
+    for (long long row = (long long)blockIdx.x * (LR_NT / 32) + warp; row < rows;
+         row += (long long)gridDim.x * (LR_NT / 32)) {
+        const long long base = row * g.nz;
+        double acc[LMAX + 1];
+#pragma unroll
+        for (int t = 0; t <= LMAX; t++) acc[t] = 0.0;
+        for (int k0 = 0; k0 < g.nz; k0 += 32 * LR_UNROLL) {
+            double rv[LR_UNROLL];
+#pragma unroll
+            for (int u = 0; u < LR_UNROLL; u++) {
+                const int k = k0 + 32 * u + lane;
+                rv[u] = k < g.nz ? dens(a, base + k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < LR_UNROLL; u++) {
+                if (rv[u] > 0.0) {
+                    const double z = z0 + (k0 + 32 * u + lane + 0.5) * g.dz;
+                    double w = rv[u];
+                    acc[0] += w;
+#pragma unroll
+                    for (int t = 1; t <= LMAX; t++) {
+                        w *= z;
+                        acc[t] += w;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t <= LMAX; t++) acc[t] = warp_sum(acc[t]);
+        if (lane == 0) {
+#pragma unroll
+            for (int t = 0; t <= LMAX; t++) zs[t * rows + row] = acc[t];
+        }
+    }
+}
+
+// Order m = blockIdx.y; each thread takes rows blockIdx.x * LR_ROWBLK +
+// threadIdx.x, + gridDim.x * LR_ROWBLK, ...; the block's sums of
+// dV N_lm Q_m^m sum_t c_lt Z_t go to its partial slots (l*l+l+m for the real
+// part, l*l+l-m for the imaginary part), which lmax_final adds in block order.
+template <int LMAX>
+__global__ void __launch_bounds__(LR_ROWBLK) lmax_rows(GravArgs a, const double *com, const double *zs)
+{
+    const Geom g = a.g;
+    const int m = blockIdx.y;
+    const long long rows = (long long)g.nx * g.ny;
+    const double xc = com[0], yc = com[1];
     double ar[LMAX + 1], ai[LMAX + 1];
 #pragma unroll
     for (int d = 0; d <= LMAX; d++) ar[d] = ai[d] = 0.0;
-    const long long rows = (long long)g.nx * g.ny;
-    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
-      const int i = (int)(row / g.ny), j = (int)(row % g.ny);
-      const double x = g.xmin + (i + 0.5) * g.dx - xc;
-      const double y = g.ymin + (j + 0.5) * g.dy - yc;
-      for (int k = lane; k < g.nz; k += 32) {
-        const long long c = row * snz + k;
-        const double r = a.rho ? a.rho[c] : (double)a.rho32[c];
-        if (!(r > 0.0)) continue;
-        const double z = g.zmin + (k + 0.5) * g.dz - zc;
-        const double dm = r * dV;
-        const double r2 = x * x + y * y + z * z;
+    for (long long row = (long long)blockIdx.x * LR_ROWBLK + threadIdx.x; row < rows;
+         row += (long long)gridDim.x * LR_ROWBLK) {
+        const int i = (int)(row / g.ny), j = (int)(row % g.ny);
+        const double x = g.xmin + (i + 0.5) * g.dx - xc;
+        const double y = g.ymin + (j + 0.5) * g.dy - yc;
+        const double rho2 = x * x + y * y;
         double smr = 1.0, smi = 0.0;      // Q_m^m
         for (int q = 1; q <= m; q++) {
             const double f = (double)(2 * q - 1);
@@ -104,47 +238,64 @@ __global__ void __launch_bounds__(32 * (LMAX + 1)) lmax_partial(GravArgs a, cons
             smr = nr;
             smi = ni;
         }
-        double pr = smr, pi = smi, ppr = 0.0, ppi = 0.0;
-        {
-            const double nrm = c_norm[m * (LM_MAX + 1) + m];
-            ar[0] += dm * (nrm * smr);
-            ai[0] += dm * (nrm * smi);
-        }
+        double Z[LMAX + 1];
 #pragma unroll
-        for (int d = 1; d <= LMAX; d++) {
-            const int l = m + d;
-            if (l > lmax) break;
-            double cr, ci;
-            if (d == 1) {
-                cr = (2 * m + 1) * z * smr;
-                ci = (2 * m + 1) * z * smi;
+        for (int t = 0; t <= LMAX; t++) Z[t] = (t <= LMAX - m) ? zs[t * rows + row] : 0.0;
+        double c1[LMAX + 1], c2[LMAX + 1];   // coefficients of p_{l-1}, p_{l-2}
+#pragma unroll
+        for (int t = 0; t <= LMAX; t++) c1[t] = c2[t] = 0.0;
+#pragma unroll
+        for (int d = 0; d <= LMAX; d++) {
+            if (d > LMAX - m) break;
+            double c0[LMAX + 1];
+#pragma unroll
+            for (int t = 0; t <= LMAX; t++) c0[t] = 0.0;
+            if (d == 0) {
+                c0[0] = 1.0;
+            } else if (d == 1) {
+                c0[1] = (double)(2 * m + 1);
             } else {
-                const double aa = (double)(2 * l - 1), bb = (double)(l + m - 1), inv = c_rinv[d];
-                cr = (aa * z * pr - bb * r2 * ppr) * inv;
-                ci = (aa * z * pi - bb * r2 * ppi) * inv;
+                const int l = m + d;
+                const double aa = (double)(2 * l - 1), bb = (double)(l + m - 1), inv = 1.0 / (double)d;
+#pragma unroll
+                for (int t = 0; t <= d; t++) {
+                    const double v1 = t >= 1 ? c1[t - 1] : 0.0;
+                    const double v3 = t >= 2 ? c2[t - 2] : 0.0;
+                    c0[t] = (aa * v1 - bb * (rho2 * c2[t] + v3)) * inv;
+                }
             }
-            ppr = pr;
-            ppi = pi;
-            pr = cr;
-            pi = ci;
-            const double nrm = c_norm[l * (LM_MAX + 1) + m];
-            ar[d] += dm * (nrm * cr);
-            ai[d] += dm * (nrm * ci);
+            double S = 0.0;
+#pragma unroll
+            for (int t = 0; t <= d; t++) S += c0[t] * Z[t];
+            ar[d] += smr * S;
+            ai[d] += smi * S;
+#pragma unroll
+            for (int t = 0; t <= LMAX; t++) {
+                c2[t] = c1[t];
+                c1[t] = c0[t];
+            }
         }
-      }
     }
+    constexpr int NW = LR_ROWBLK / 32;
+    __shared__ double red[NW][2 * (LMAX + 1)];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int d = 0; d <= LMAX; d++) {
-        double vr = ar[d], vi = ai[d];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            vr += __shfl_xor_sync(0xffffffffu, vr, o);
-            vi += __shfl_xor_sync(0xffffffffu, vi, o);
+        const double vr = warp_sum(ar[d]), vi = warp_sum(ai[d]);
+        if (lane == 0) {
+            red[warp][2 * d] = vr;
+            red[warp][2 * d + 1] = vi;
         }
-        const int l = m + d;
-        if (lane == 0 && l <= lmax) {
-            a.scratch[(long long)blockIdx.x * LM_NC + l * l + l + m] = vr;
-            if (m > 0) a.scratch[(long long)blockIdx.x * LM_NC + l * l + l - m] = vi;
+    }
+    __syncthreads();
+    const int q = threadIdx.x;
+    if (q < 2 * (LMAX + 1)) {
+        const int d = q >> 1, l = m + d;
+        if (l <= LMAX && (m > 0 || !(q & 1))) {
+            double s = 0.0;
+            for (int w = 0; w < NW; w++) s += red[w][q];
+            const double f = c_norm[l * (LM_MAX + 1) + m] * (g.dx * g.dy * g.dz);
+            a.scratch[(long long)blockIdx.x * LM_NC + l * l + l + ((q & 1) ? -m : m)] = f * s;
         }
     }
 }
@@ -223,53 +374,47 @@ cudaError_t ensure_norm()
         }
     cudaError_t e = cudaMemcpyToSymbol(c_norm, h, sizeof h);
     if (e != cudaSuccess) return e;
-    double rinv[LM_MAX + 1];
-    for (int d = 0; d <= LM_MAX; d++) rinv[d] = d > 0 ? 1.0 / (double)d : 0.0;
-    e = cudaMemcpyToSymbol(c_rinv, rinv, sizeof rinv);
-    if (e == cudaSuccess && dev < 64) g_norm_ready[dev] = true;
-    return e;
+    if (dev < 64) g_norm_ready[dev] = true;
+    return cudaSuccess;
 }
 
 }  // namespace
 
-// centre of mass first (tree), then the solid-harmonic moments about it
+// centre of mass, the rows' z-power sums about it, then the solid-harmonic
+// moments row by row.  Scratch: partial sums at [0, LM_SCRATCH0), the z-power
+// sums (lmax + 1 per row) after it.
 cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
 {
     if (a.lmax < 1 || a.lmax > LM_MAX) return cudaErrorInvalidValue;
-
+    const long long rows = (long long)a.g.nx * a.g.ny;
+    if (a.scratch_len < LM_SCRATCH0 + rows * (LM_MAX + 1)) return cudaErrorInvalidValue;
     cudaError_t e = ensure_norm();
     if (e != cudaSuccess) return e;
-    GravArgs t = a;
-    e = grav_moments_tree(t, s);       // M, COM, Q (Q unused here)
-    if (e != cudaSuccess) return e;
-    // blocks: every SM filled to its occupancy for this l_max
-    static int nb_cache[LM_MAX + 1] = { 0 };
-    int nb = nb_cache[a.lmax];
-    auto launch = [&](auto kern) -> cudaError_t {
-        if (!nb) {
-            int per = 0;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 32 * (a.lmax + 1), 0) != cudaSuccess ||
-                per < 1)
-                per = 1;
-            nb = std::min(148 * per, (int)(a.scratch_len / LM_NC));
-            nb_cache[a.lmax] = nb;
-        }
-        kern<<<nb, 32 * (a.lmax + 1), 0, s>>>(a, a.sc->moments + 1);
+    constexpr int NCOM = 592;   // 4 CTAs of 8 warps per SM
+    lmax_com_partial<<<NCOM, LR_NT, 0, s>>>(a);
+    lmax_com_final<<<1, 32, 0, s>>>(a, NCOM);
+    const double *com = a.sc->moments + 1;
+    double *zs = a.scratch + LM_SCRATCH0;
+    const int nzb = (int)std::min<long long>((rows + LR_NT / 32 - 1) / (LR_NT / 32), 148LL * 8);
+    const int nb = (int)std::min<long long>((rows + LR_ROWBLK - 1) / LR_ROWBLK, LM_SCRATCH0 / LM_NC);
+    auto launch = [&](auto zk, auto rk) -> cudaError_t {
+        zk<<<nzb, LR_NT, 0, s>>>(a, com, zs);
+        rk<<<dim3(nb, a.lmax + 1), LR_ROWBLK, 0, s>>>(a, com, zs);
         return cudaGetLastError();
     };
     switch (a.lmax) {
-    case 1: e = launch(lmax_partial<1>); break;
-    case 2: e = launch(lmax_partial<2>); break;
-    case 3: e = launch(lmax_partial<3>); break;
-    case 4: e = launch(lmax_partial<4>); break;
-    case 5: e = launch(lmax_partial<5>); break;
-    case 6: e = launch(lmax_partial<6>); break;
-    case 7: e = launch(lmax_partial<7>); break;
-    case 8: e = launch(lmax_partial<8>); break;
-    case 9: e = launch(lmax_partial<9>); break;
-    case 10: e = launch(lmax_partial<10>); break;
-    case 11: e = launch(lmax_partial<11>); break;
-    default: e = launch(lmax_partial<12>); break;
+    case 1: e = launch(lmax_zsums<1>, lmax_rows<1>); break;
+    case 2: e = launch(lmax_zsums<2>, lmax_rows<2>); break;
+    case 3: e = launch(lmax_zsums<3>, lmax_rows<3>); break;
+    case 4: e = launch(lmax_zsums<4>, lmax_rows<4>); break;
+    case 5: e = launch(lmax_zsums<5>, lmax_rows<5>); break;
+    case 6: e = launch(lmax_zsums<6>, lmax_rows<6>); break;
+    case 7: e = launch(lmax_zsums<7>, lmax_rows<7>); break;
+    case 8: e = launch(lmax_zsums<8>, lmax_rows<8>); break;
+    case 9: e = launch(lmax_zsums<9>, lmax_rows<9>); break;
+    case 10: e = launch(lmax_zsums<10>, lmax_rows<10>); break;
+    case 11: e = launch(lmax_zsums<11>, lmax_rows<11>); break;
+    default: e = launch(lmax_zsums<12>, lmax_rows<12>); break;
     }
     if (e != cudaSuccess) return e;
     lmax_final<<<1, 256, 0, s>>>(a, nb);

@@ -212,6 +212,11 @@ int hc_unet_loss_grad(hc_ctx *ctx, int nx, int ny, int nz, const float *x, const
 /* Predictions per solve (1..8, default 1): after an accepted prediction the
  * network is applied again to the residual it left, until one is rejected. */
 int hc_set_unet_passes(hc_ctx *ctx, int passes);
+/* Correction cycles of a mixed-precision solve that start from a prediction
+ * (1..8, default 2): the first from the step's residual, the second from the
+ * smooth residual the first cycle's sweeps left; each prediction is kept only
+ * if it lowers max|delta|. */
+int hc_set_unet_cycles(hc_ctx *ctx, int cycles);
 
 /* Diagnostics of the tensor-core convolution kernels (no reference
  * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16

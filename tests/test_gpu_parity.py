@@ -142,9 +142,11 @@ def test_tree_moments_close():
     np.testing.assert_allclose(m_g, m_o, rtol=1e-12, atol=1e-14 * abs(m_o[0]))
 
 
-@pytest.mark.parametrize("lmax", [2, 4, 8, 12])
-def test_lmax_boundary_matches_oracle(lmax):
-    shape = (20, 22, 18)
+@pytest.mark.parametrize("lmax,shape", [(2, (20, 22, 18)), (4, (20, 22, 18)), (8, (20, 22, 18)),
+                                         (12, (20, 22, 18)), (8, (8, 6, 300)), (12, (30, 28, 33))])
+def test_lmax_boundary_matches_oracle(lmax, shape):
+    """Row-factored moments (rows longer than one pass of a warp, odd sizes)
+    against the oracle's direct per-cell sums, and the boundary values."""
     q0, _ = ics.polytrope_n1(shape, R=0.25, centre=(0.45, 0.55, 0.5))
     rho = q0[0] * (1.0 + 0.3 * (ics.centres(shape, (0, 0, 0), (1, 1, 1))[0] > 0.5))
     o = OracleSim(*shape, G=1.0, tol=1e-8, max_iter=1, lmax=lmax)
