@@ -278,9 +278,11 @@ def reference_sample(q0, p, sor_iters=10):
 
 
 # DRAM bytes (read + write) per grid cell of one launch, from ncu captures of
-# the 256^3 workload (profiles/sor_split_kernel_fp{32,64}_stellar_explosion_256.txt),
-# keyed by kernel and word size.
-NCU_DRAM_BYTES_PER_CELL = {("sor_split_kernel", 4): 6.47, ("sor_split_kernel", 8): 14.38}
+# the 256^3 workload (profiles/sor_split_vec_kernel_fp32_stellar_explosion_256.txt,
+# profiles/sor_split_kernel_fp64_stellar_explosion_256.txt), keyed by kernel.
+NCU_DRAM_BYTES_PER_CELL = {"sor_split_vec_kernel": 6.47, "sor_split_kernel": 14.38}
+# the colour sweep each precision runs (FP32: 16-byte vector sweeps)
+SOR_KERNEL = {4: "sor_split_vec_kernel", 8: "sor_split_kernel"}
 
 REF_ITERS_FILE = os.path.join(ROOT, "hydrocode_astro1_b200", "data", "fp64_iterations.json")
 
@@ -362,25 +364,29 @@ def main_ours(args):
     s = r["solver"]
     fp64 = variant.startswith("fp64")
 
-    # roofline of the dominant kernel: one colour sweep of the colour-split SOR
-    # (sor_split_kernel).  Algorithmic bytes: half an iteration's 24 B/cell
-    # (FP64 phi read + write, rho read) or 12 B/cell (FP32 e read + write, r
-    # read) over the interior cells.
+    # roofline of the dominant kernel: one colour sweep of the colour-split SOR.
+    # Algorithmic bytes: half an iteration's 24 B/cell (FP64 phi read + write,
+    # rho read) or 12 B/cell (FP32 e read + write, r read) over the interior
+    # cells.  Launch time: the SOR family's CUDA-event time over the sweeps
+    # that ran (two per iteration); it also holds the convergence checks and
+    # the sweeps queued past convergence that return at once, so it is an
+    # upper bound of the sweep time.
     interior = (p["shape"][0] - 2) * (p["shape"][1] - 2) * (p["shape"][2] - 2)
     word = 8 if fp64 else 4
     bytes_per_launch = interior * 3 * word / 2.0
-    sor_launches = max(tm["sor_launches"], 1)
-    sor_avg_ms = tm["sor_ms"] / sor_launches
+    sweeps = max(2 * sum(r["iters"]), 1)
+    sor_avg_ms = tm["sor_ms"] / sweeps
     pk, pk_kind = peaks()
     achieved = bytes_per_launch / (sor_avg_ms / 1e3) / 1e9 if sor_avg_ms > 0 else 0.0
     shares = {k: tm[k] for k in ("hydro_ms", "bc_ms", "sor_ms", "residual_ms", "moments_ms", "unet_ms")}
-    traffic = NCU_DRAM_BYTES_PER_CELL.get(("sor_split_kernel", word))
-    roofline = {"bound": "hbm", "kernel": "sor_split_kernel", "achieved": achieved, "peak": pk, "unit": "GB/s",
+    kname = SOR_KERNEL[word]
+    traffic = NCU_DRAM_BYTES_PER_CELL.get(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": pk, "unit": "GB/s",
                 "frac": achieved / pk, "peak_kind": pk_kind,
                 "traffic": traffic * ncell if traffic else None,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "layout_bytes_per_launch": 4 * word * ncell / 2.0,
-                "avg_launch_ms": sor_avg_ms, "launches": tm["sor_launches"]}
+                "avg_launch_ms": sor_avg_ms, "sweeps": sweeps, "launches": tm["sor_launches"]}
     hydro_bytes = interior * (48 if not fp64 else 88)
     hydro_avg = tm["hydro_ms"] / max(tm["hydro_launches"], 1)
     hydro_roof = {"kernel": "hydro_interior", "achieved": hydro_bytes / (hydro_avg / 1e3) / 1e9 if hydro_avg else 0,

@@ -141,18 +141,18 @@ __global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a)
 }
 
 // M = dV S0 and the centre of mass (box centre when there is no mass), as
-// the reference's monopole pass stores them
-__global__ void lmax_com_final(GravArgs a, int nparts)
+// the reference's monopole pass stores them.  Warp q adds the partials of
+// sum q (lane-strided, then a fixed butterfly).
+__global__ void __launch_bounds__(128) lmax_com_final(GravArgs a, int nparts)
 {
     __shared__ double v[4];
-    const int q = threadIdx.x;
-    if (q < 4) {
-        double s = 0.0;
-        for (int b = 0; b < nparts; b++) s += a.scratch[(long long)b * 4 + q];
-        v[q] = s;
-    }
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int b = lane; b < nparts; b += 32) s += a.scratch[(long long)b * 4 + q];
+    s = warp_sum(s);
+    if (lane == 0) v[q] = s;
     __syncthreads();
-    if (q != 0) return;
+    if (threadIdx.x != 0) return;
     const Geom g = a.g;
     a.sc->moments[0] = v[0] * (g.dx * g.dy * g.dz);
     if (v[0] > 0.0) {
@@ -300,20 +300,16 @@ __global__ void __launch_bounds__(LR_ROWBLK) lmax_rows(GravArgs a, const double 
     }
 }
 
-__global__ void lmax_final(GravArgs a, int nparts)
+// one warp per coefficient: the blocks' partials, lane-strided, then a fixed
+// butterfly (deterministic)
+__global__ void __launch_bounds__(32) lmax_final(GravArgs a, int nparts)
 {
-    const int nc = (a.lmax + 1) * (a.lmax + 1);
-    for (int t = threadIdx.x; t < nc; t += blockDim.x) {
-        double s = 0.0;
-        for (int b = 0; b < nparts; b++) s += a.scratch[(long long)b * LM_NC + t];
-        a.mom[4 + t] = s;
-    }
-    if (threadIdx.x == 0) {
-        a.mom[0] = a.sc->moments[0];
-        a.mom[1] = a.sc->moments[1];
-        a.mom[2] = a.sc->moments[2];
-        a.mom[3] = a.sc->moments[3];
-    }
+    const int t = blockIdx.x, lane = threadIdx.x;
+    double s = 0.0;
+    for (int b = lane; b < nparts; b += 32) s += a.scratch[(long long)b * LM_NC + t];
+    s = warp_sum(s);
+    if (lane == 0) a.mom[4 + t] = s;
+    if (t == 0 && lane < 4) a.mom[lane] = a.sc->moments[lane];
 }
 
 __device__ __forceinline__ double eval_lmax(double x, double y, double z, int lmax,
@@ -392,7 +388,7 @@ cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
     if (e != cudaSuccess) return e;
     constexpr int NCOM = 592;   // 4 CTAs of 8 warps per SM
     lmax_com_partial<<<NCOM, LR_NT, 0, s>>>(a);
-    lmax_com_final<<<1, 32, 0, s>>>(a, NCOM);
+    lmax_com_final<<<1, 128, 0, s>>>(a, NCOM);
     const double *com = a.sc->moments + 1;
     double *zs = a.scratch + LM_SCRATCH0;
     const int nzb = (int)std::min<long long>((rows + LR_NT / 32 - 1) / (LR_NT / 32), 148LL * 8);
@@ -417,7 +413,7 @@ cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
     default: e = launch(lmax_zsums<12>, lmax_rows<12>); break;
     }
     if (e != cudaSuccess) return e;
-    lmax_final<<<1, 256, 0, s>>>(a, nb);
+    lmax_final<<<(a.lmax + 1) * (a.lmax + 1), 32, 0, s>>>(a, nb);
     return cudaGetLastError();
 }
 
