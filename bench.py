@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--unet-passes", type=int, default=1, help="learned-start predictions per solve")
+    ap.add_argument("--unet-weights", default=None, help="weight file of the learned start (default: the committed one)")
+    ap.add_argument("--sor-depth", type=int, default=None,
+                    help="FP32 correction sweeps: 0 per-colour split sweeps, -2 two iterations per pass")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="skip the FP32 arm without the learned warm start")
     return ap.parse_args()
@@ -149,6 +152,8 @@ def solver_kwargs(p, variant, device):
     import hydrocode_astro1_b200 as hc
     kw = dict(lo=p["lo"], hi=p["hi"], gamma=p["gamma"], G=p["G"], bc=p["bc"], lmax=p["lmax"],
               cfl=p["cfl"], tol=1e-8, max_iter=2_000_000, omega=1.5, device=device)
+    if SOR_DEPTH is not None and not variant.startswith("fp64"):
+        kw["sor_depth"] = SOR_DEPTH
     if variant == "fp64":
         kw.update(precision=hc.FP64, lmax=p["lmax"], moment_order=hc.MOMENTS_TREE)
     elif variant == "fp64_tree":
@@ -164,6 +169,7 @@ def solver_kwargs(p, variant, device):
 # `python -m hydrocode_astro1_b200.train_unet` from solves of this workload
 # with another density-noise seed (7); the benchmark run uses seed 42.
 UNET_WEIGHTS = os.path.join(ROOT, "hydrocode_astro1_b200", "data", "unet_stellar_explosion_256.bin")
+SOR_DEPTH = None   # FP32 correction sweep mode (library default when None)
 UNET_PASSES = 1
 
 
@@ -346,8 +352,11 @@ def main_reference(args):
 def main_ours(args):
     import numpy as np
 
-    global UNET_PASSES
+    global UNET_PASSES, UNET_WEIGHTS, SOR_DEPTH
+    SOR_DEPTH = args.sor_depth
     UNET_PASSES = args.unet_passes
+    if args.unet_weights:
+        UNET_WEIGHTS = os.path.abspath(args.unet_weights)
 
     import hydrocode_astro1_b200 as hc
     world, rank, local, dist = dist_setup(args)

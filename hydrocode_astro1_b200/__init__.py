@@ -106,6 +106,7 @@ CAPI = {
     "hc_unet_samples": (C.c_int, [C.c_void_p]),
     "hc_set_unet_passes": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_cycles": (C.c_int, [C.c_void_p, C.c_int]),
+    "hc_set_unet_record_cycle": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_unet_train": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint, C.POINTER(C.c_double)]),
     "hc_unet_loss_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float),
@@ -349,6 +350,10 @@ class HydroSolver3D:
     def unet_cycles(self, n):
         """Correction cycles that start from the network's prediction (default 2)."""
         _check(self.L.hc_set_unet_cycles(self.h, int(n)), "hc_set_unet_cycles")
+
+    def unet_record_cycle(self, c):
+        """With collection on: the correction cycle whose residual is recorded."""
+        _check(self.L.hc_set_unet_record_cycle(self.h, int(c)), "hc_set_unet_record_cycle")
 
     def unet_train(self, steps, lr=1e-3, seed=0):
         loss = C.c_double(0.0)

@@ -101,6 +101,7 @@ struct hc_ctx {
     int debug;                   // HC_DEBUG=1: per-solve progress on stderr
     int unet_passes;             // learned-start predictions per solve (>= 1)
     int unet_cycles;             // correction cycles that start from a prediction (0: 2)
+    int unet_record_cycle;       // the cycle whose residual is recorded for training (0: 1)
 };
 
 static cudaEvent_t ev_get(hc_ctx *c)
@@ -652,11 +653,14 @@ static int sor_fp64(hc_ctx *c, const double *rho)
 int hc_sor_mixed(hc_ctx *c, const float *rho32)
 {
     GravArgs a = grav_args(c, nullptr, rho32);
-    // sor_depth 0 (default): colour-split sweeps on e and r; -1: one in-place
-    // kernel per colour on the natural layout; >= 1: wavefront passes of that
-    // many FP32 iterations per HBM pass (temporal blocking)
-    const bool split = c->cfg.sor_depth == 0 && c->g.nz >= 3;
-    const int depth = c->cfg.sor_depth == 0 ? -1 : c->cfg.sor_depth;
+    // sor_depth 0 (default): colour-split sweeps on e and r; -2: colour-split,
+    // two iterations per HBM pass (temporal blocking, out of place between
+    // e32 and e32b; colour-split sweeps where the tiling does not fit); -1:
+    // one in-place kernel per colour on the natural layout; >= 1: wavefront
+    // passes of that many FP32 iterations per HBM pass on the natural layout
+    const bool split = (c->cfg.sor_depth == 0 || c->cfg.sor_depth == -2) && c->g.nz >= 3;
+    const bool wave2 = split && c->cfg.sor_depth == -2 && mixed_wave_split_ok(c->g);
+    const int depth = wave2 ? 2 : (split ? -1 : c->cfg.sor_depth);
     int rc = ensure_res(c, a.max_iter);
     if (rc) return rc;
     a.res = c->res;
@@ -694,12 +698,13 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         // after the hydro update); the second's is what the first cycle's
         // sweeps left (smooth), where the prediction removes the slow modes
         // that the remaining sweeps would spend most of their iterations on.
-        // With sample collection on, the first cycle's residual and phi are
-        // recorded for training.
+        // With sample collection on, the residual and phi at the start of
+        // cycle unet_record_cycle are recorded for training.
         const int ucycles = c->unet_cycles > 0 ? c->unet_cycles : 2;
-        if (cycles <= ucycles && split && c->unet && std::isfinite(dmax)) {
-            const bool predict = c->cfg.warm_start == HC_WARM_UNET && unet_has_weights(c->unet);
-            const bool rec = cycles == 1 && unet_collecting(c->unet);
+        const int rcycle = c->unet_record_cycle > 0 ? c->unet_record_cycle : 1;
+        if ((cycles <= ucycles || cycles == rcycle) && split && c->unet && std::isfinite(dmax)) {
+            const bool predict = cycles <= ucycles && c->cfg.warm_start == HC_WARM_UNET && unet_has_weights(c->unet);
+            const bool rec = cycles == rcycle && unet_collecting(c->unet);
             if (predict || rec) {
                 {
                     FamTimer t(c, FAM_UNET);
@@ -760,6 +765,9 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));
         CK(grav_reset_slots(a, 0, budget + 8, c->s));
         float *eb[2] = { c->e32, c->e32b };
+        // the passes write every interior cell of their output; its boundary
+        // cells (zero for the correction) come from here
+        if (wave2) CK(cudaMemsetAsync(c->e32b, 0, (size_t)split_len(c->g) * sizeof(float), c->s));
         int it = 0, done = 0, last = 0, batch = 16, processed = 0, best_it = 0;
         double best = 1e300;
         if (!c->hslots && cudaMallocHost((void **)&c->hslots, 512 * sizeof(double)) != cudaSuccess)
@@ -768,7 +776,14 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
             int end = std::min(budget, it + batch);
             {
                 FamTimer t(c, FAM_SOR);
-                if (split) {
+                if (wave2) {
+                    for (int q = it; q < end; q += 2) {
+                        CK(mixed_sor32_split_pass(a, eb[(q / 2) & 1], eb[((q / 2) + 1) & 1], c->r32, q, thresh, c->s));
+                        c->launches += 1;
+                        c->sor_launches += 1;
+                    }
+                    end = it + ((end - it + 1) / 2) * 2;
+                } else if (split) {
                     for (int q = it; q < end; q++) {
                         CK(mixed_sor32_split(a, c->e32, c->r32, 0, q, thresh, c->s));
                         CK(mixed_sor32_split(a, c->e32, c->r32, 1, q, thresh, c->s));
@@ -820,7 +835,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         const int used = done ? last : processed;
         total += used;
         // the correction is in eb[passes % 2] for the blocked sweeps
-        const float *efinal = (split || depth < 0) ? c->e32 : eb[(used / depth) & 1];
+        const float *efinal = ((split && !wave2) || depth < 0) ? c->e32 : eb[(used / depth) & 1];
         {
             FamTimer t(c, FAM_RES);
             CK(cudaMemsetAsync(&c->sc->resid_bits, 0, sizeof(unsigned long long), c->s));
@@ -1363,5 +1378,12 @@ extern "C" int hc_set_unet_cycles(hc_ctx *c, int cycles)
 {
     if (!c || cycles < 1 || cycles > 8) return set_err(HC_ERR_ARG, "cycles must be 1..8");
     c->unet_cycles = cycles;
+    return HC_OK;
+}
+
+extern "C" int hc_set_unet_record_cycle(hc_ctx *c, int cycle)
+{
+    if (!c || cycle < 1 || cycle > 8) return set_err(HC_ERR_ARG, "cycle must be 1..8");
+    c->unet_record_cycle = cycle;
     return HC_OK;
 }

@@ -16,6 +16,7 @@
 #include "hc_internal.cuh"
 #include "hc_math.cuh"
 #include "sor_split.cuh"
+#include "sor_wave_split.cuh"
 
 namespace hc {
 
@@ -614,6 +615,76 @@ cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int col
 cudaError_t mixed_check(const GravArgs &a, int iter, double thresh, cudaStream_t s)
 {
     check32_kernel<<<1, 1, 0, s>>>(a, iter, thresh);
+    return cudaGetLastError();
+}
+
+// Tiling of the two-iteration passes: the largest window (BJ <= 8 owned rows)
+// that fits shared memory, and the row tiles x plane chunks that fill the SMs
+// with one CTA each at the least recomputed halo.
+static bool wave_split_plan(const Geom &g, int &BJ, int &L, int &jt, int &ch)
+{
+    const Split sp = make_split(g);
+    if (g.nz < 3 || g.nx < 3 || g.ny < 3 || sp.H % 4) return false;
+    int dev = 0, nsm = 148, optin = 227 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    double best = 1e300;
+    bool ok = false;
+    for (int bj = 8; bj >= 4; bj--) {
+        if (wave_split_smem(bj + 2 * WV_NH, sp.H) + 2 * (WV_THREADS / 32) * sizeof(float) > (size_t)optin) continue;
+        const int t = (g.ny - 2 + bj - 1) / bj;
+        const int c = std::max(1, (int)std::lround((double)nsm / t));
+        const int l = (g.nx - 2 + c - 1) / c;
+        const int cc = (g.nx - 2 + l - 1) / l;
+        const long long ctas = (long long)t * cc;
+        const long long waves = (ctas + nsm - 1) / nsm;
+        const double eff = (double)ctas / (double)(waves * nsm);
+        const double halo = (4.0 * bj + 12.0) / (4.0 * bj) * (l + 6.0) / l;
+        const double cost = halo / eff;
+        if (cost < best) {
+            best = cost;
+            BJ = bj;
+            L = l;
+            jt = t;
+            ch = cc;
+            ok = true;
+        }
+    }
+    return ok;
+}
+
+bool mixed_wave_split_ok(const Geom &g)
+{
+    int BJ, L, jt, ch;
+    return wave_split_plan(g, BJ, L, jt, ch);
+}
+
+cudaError_t mixed_sor32_split_pass(const GravArgs &a, const float *ein, float *eout, const float *r32, int iter0,
+                                   double thresh, cudaStream_t s)
+{
+    int BJ = 0, L = 0, jt = 0, ch = 0;
+    if (!wave_split_plan(a.g, BJ, L, jt, ch)) return cudaErrorInvalidValue;
+    const Split sp = make_split(a.g);
+    if (sp.cs + 2LL * sp.ny * sp.H >= (1LL << 31)) return cudaErrorInvalidValue;
+    const size_t smem = wave_split_smem(BJ + 2 * WV_NH, sp.H);
+    static size_t attr_bytes[64] = { 0 };
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 64 || smem > attr_bytes[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(sor_wave_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        if (dev < 64) attr_bytes[dev] = smem;
+    }
+    const MixConst mc = mix_const(a);
+    SorCoef<float> cf;
+    cf.cx = mc.cx;
+    cf.cy = mc.cy;
+    cf.cz = mc.cz;
+    cf.om = mc.om;
+    sor_wave_split_kernel<<<dim3(jt, ch), WV_THREADS, smem, s>>>(ein, eout, r32, sp, cf, BJ, L, a.res, iter0, thresh,
+                                                                 a.sc);
     return cudaGetLastError();
 }
 

@@ -163,6 +163,10 @@ cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, i
 cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int color, int iter,
                         double thresh, cudaStream_t s);
 cudaError_t mixed_check(const GravArgs &a, int iter, double thresh, cudaStream_t s);
+// two FP32 correction iterations per pass on the colour-split layout, ein -> eout
+bool mixed_wave_split_ok(const Geom &g);
+cudaError_t mixed_sor32_split_pass(const GravArgs &a, const float *ein, float *eout, const float *r32, int iter0,
+                                   double thresh, cudaStream_t s);
 }  // namespace hc
 
 namespace hc {

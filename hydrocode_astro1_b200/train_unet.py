@@ -4,8 +4,11 @@
         --solves 25 --train-steps 2000 --out hydrocode_astro1_b200/data/unet_stellar_explosion_256.bin
 
 Runs `solves` steps of the problem in FP32 + mixed precision with the
-previous-potential warm start (the plain method), recording one (residual,
-converged correction) pair per Poisson solve on the device; then trains the
+previous-potential warm start (the plain method) for each recorded cycle,
+recording one (residual, converged correction) pair per Poisson solve on the
+device -- the residual at the start of the first correction cycle (after the
+hydro update) or of the second (the smooth remainder the first cycle's sweeps
+left), the correction from there to the converged potential; then trains the
 network on those pairs with the library's own tensor-core forward/backward
 kernels and Adam (hc_unet_train), and writes the weight file plus a JSON
 report (same name, .json) with the training losses.  The density noise seed
@@ -53,17 +56,22 @@ def main():
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--init-seed", type=int, default=1)
+    ap.add_argument("--record-cycles", default="1",
+                    help="correction cycles to record, `solves` steps each, in this order")
     ap.add_argument("--out", required=True)
     a = ap.parse_args()
     t0 = time.time()
     q, p = make(a.problem, a.n, a.seed)
     s = solver(q, p)
-    s.unet_collect(a.solves + 1)
+    cycles = [int(c) for c in a.record_cycles.split(",")]
+    s.unet_collect(a.solves * len(cycles) + 1)
     s.unet_init(a.init_seed)
     iters = []
-    for _ in range(a.solves):
-        s.step(1)
-        iters.append(s.diagnostics()["last_iterations"])
+    for c in cycles:
+        s.unet_record_cycle(c)
+        for _ in range(a.solves):
+            s.step(1)
+            iters.append(s.diagnostics()["last_iterations"])
     t_collect = time.time() - t0
     losses = []
     chunk = max(1, a.train_steps // 10)
@@ -77,7 +85,8 @@ def main():
     t_train = time.time() - t0 - t_collect
     s.unet_save_file(a.out)
     tm = s.timing()
-    report = {"problem": a.problem, "n": a.n, "seed": a.seed, "solves": a.solves, "samples": s.unet_samples(),
+    report = {"problem": a.problem, "n": a.n, "seed": a.seed, "solves": a.solves, "record_cycles": cycles,
+              "samples": s.unet_samples(),
               "sor_iterations": iters, "train_steps": a.train_steps, "lr": a.lr,
               "loss_per_chunk": losses, "collect_s": t_collect, "train_s": t_train,
               "unet_device_ms": tm["unet_ms"], "params": hc.lib().hc_unet_param_count()}

@@ -217,6 +217,9 @@ int hc_set_unet_passes(hc_ctx *ctx, int passes);
  * smooth residual the first cycle's sweeps left; each prediction is kept only
  * if it lowers max|delta|. */
 int hc_set_unet_cycles(hc_ctx *ctx, int cycles);
+/* With collection on (hc_unet_collect): the correction cycle whose starting
+ * residual is recorded as a training sample (1..8, default 1). */
+int hc_set_unet_record_cycle(hc_ctx *ctx, int cycle);
 
 /* Diagnostics of the tensor-core convolution kernels (no reference
  * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16

@@ -206,7 +206,7 @@ def test_sor_layouts_chunks_bitwise(shape, depth):
     assert_bitwise(s.phi(), o.phi, "phi")
 
 
-@pytest.mark.parametrize("depth", [0, -1, 1, 2, 4])
+@pytest.mark.parametrize("depth", [0, -2, -1, 1, 2, 4])
 def test_mixed_precision_poisson_converges(depth):
     """FP64 residual + FP32 correction sweeps reach the same tolerance; the
     potential agrees with the FP64 solution to the accuracy the tolerance
@@ -229,6 +229,28 @@ def test_mixed_precision_poisson_converges(depth):
     assert o.sweep_norm(phi, r32) < tol
     # distance to the converged FP64 potential (error amplification ~ N^2)
     assert np.abs(phi - o.phi).max() < 2e-4 * np.abs(o.phi).max()
+
+
+@pytest.mark.parametrize("shape", [(40, 37, 72), (130, 20, 32), (24, 60, 40), (70, 70, 64)])
+def test_mixed_two_iteration_passes_match_sweeps(shape):
+    """The colour-split passes of two iterations each (sor_depth -2: row tiles,
+    plane chunks, recomputed halo rows and planes, out of place) give the
+    iterates of the per-colour sweeps: after the same even number of
+    correction iterations the potentials agree to FP32 rounding."""
+    q0, gam = ics.polytrope_n1(shape, R=0.3)
+    phis, norms = [], []
+    for depth in (0, -2):
+        s = hc.HydroSolver3D(shape, G=1.0, gamma=gam, tol=1e-30, max_iter=30, precision=hc.FP32,
+                             moment_order=hc.MOMENTS_TREE, sor_depth=depth)
+        s.set_state(q0.astype(np.float32).astype(np.float64))
+        s.gravity_solve()
+        d = s.diagnostics()
+        assert d["last_iterations"] == 30, d
+        phis.append(s.phi())
+        norms.append(d["last_residual"])
+    diff = np.abs(phis[0] - phis[1]).max()
+    assert diff <= 1e-6 * np.abs(phis[0]).max(), diff
+    assert abs(norms[0] - norms[1]) <= 1e-5 * norms[0], norms
 
 
 def test_fp32_sod_close_to_fp64():
