@@ -45,6 +45,9 @@
 #ifndef HC_SPLIT_VEC_MINB64
 #define HC_SPLIT_VEC_MINB64 2
 #endif
+#ifndef HC_SOR_PDL
+#define HC_SOR_PDL 1
+#endif
 #ifndef HC_SPLIT_SNAKE
 #define HC_SPLIT_SNAKE 1
 #endif
@@ -73,6 +76,43 @@ inline Split make_split(const Geom &g)
 
 constexpr int SPLIT_BX = 32, SPLIT_BY = 8;
 
+// Programmatic dependent launch: a sweep launched with programmatic stream
+// serialisation may be scheduled while the previous sweep's last CTAs still
+// run; griddepcontrol.wait holds it until that grid has completed and its
+// writes are visible, so nothing is read early.  Releasing the dependents at
+// once lets the next sweep's CTAs take SM slots as this grid's last wave
+// drains (they cannot crowd out this grid: its last CTAs are already
+// resident when the release of every CTA completes).  In a kernel launched
+// without the attribute both instructions do nothing.
+__device__ __forceinline__ void pdl_wait_and_release()
+{
+#if HC_SOR_PDL
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
+template <typename K, typename... Args>
+cudaError_t launch_pdl(K kernel, dim3 grid, dim3 block, cudaStream_t s, Args... args)
+{
+#if HC_SOR_PDL
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+#else
+    kernel<<<grid, block, 0, s>>>(args...);
+    return cudaGetLastError();
+#endif
+}
+
 // One thread owns the column (j, m) over NI consecutive planes i0..i0+NI-1:
 // every operand of the NI updates is loaded first (6 NI + 2 independent
 // loads in flight per thread), then the updates run and are stored.  Offsets
@@ -86,6 +126,7 @@ sor_split_kernel(T *__restrict__ own, const T *__restrict__ oth, const S *__rest
                  SorCoef<T> cf, int colour, double *res, int iter, double thresh, DevScalars *sc)
 {
     __shared__ double wmax[SPLIT_BX * SPLIT_BY / 32];
+    pdl_wait_and_release();
     if (*(volatile int *)&sc->done) return;
     if (colour == 0 && iter > 0) {
         const double prev = __longlong_as_double(*reinterpret_cast<const volatile long long *>(res + iter - 1));
@@ -201,6 +242,7 @@ sor_split_vec_kernel(T *__restrict__ own, const T *__restrict__ oth, const T *__
     constexpr int V = Pack<T>::V;
     using P = Pack<T>;
     __shared__ double wmax[SPLIT_BX * SPLIT_BY / 32];
+    pdl_wait_and_release();
     if (*(volatile int *)&sc->done) return;
     if (colour == 0 && iter > 0) {
         const double prev = __longlong_as_double(*reinterpret_cast<const volatile long long *>(res + iter - 1));
@@ -340,15 +382,14 @@ cudaError_t launch_sor_split(T *base, const S *src, const Split &sp, const SorCo
         ((uintptr_t)base | (uintptr_t)src) % 16 == 0) {
         constexpr int VNI = HC_SPLIT_VEC_NI, VMINB = sizeof(T) == 8 ? HC_SPLIT_VEC_MINB64 : HC_SPLIT_VEC_MINB32;
         dim3 grid((sp.H / V + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + VNI - 1) / VNI);
-        sor_split_vec_kernel<T, VNI, VMINB><<<grid, dim3(SPLIT_BX, SPLIT_BY), 0, s>>>(
-            own, oth, reinterpret_cast<const T *>(src) + (size_t)colour * sp.cs, sp, cf, colour, res, iter, thresh, sc);
-        return cudaGetLastError();
+        return launch_pdl(sor_split_vec_kernel<T, VNI, VMINB>, grid, dim3(SPLIT_BX, SPLIT_BY), s, own, oth,
+                          reinterpret_cast<const T *>(src) + (size_t)colour * sp.cs, sp, cf, colour, res, iter, thresh,
+                          sc);
     }
 #endif
     dim3 grid((sp.H + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + NI - 1) / NI);
-    sor_split_kernel<T, S, NI, MINB><<<grid, dim3(SPLIT_BX, SPLIT_BY), 0, s>>>(own, oth, src + (size_t)colour * sp.cs, sp,
-                                                                         cf, colour, res, iter, thresh, sc);
-    return cudaGetLastError();
+    return launch_pdl(sor_split_kernel<T, S, NI, MINB>, grid, dim3(SPLIT_BX, SPLIT_BY), s, own, oth,
+                      src + (size_t)colour * sp.cs, sp, cf, colour, res, iter, thresh, sc);
 }
 
 }  // namespace hc
