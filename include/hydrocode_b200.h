@@ -89,8 +89,12 @@ typedef struct hc_config {
     double omega;            /* SOR relaxation (default 1.5) */
     double tol;              /* SOR tolerance on max |phi_GS - phi_old| */
     int max_iter;
-    int sor_depth;           /* SOR iterations per HBM pass (temporal blocking);
-                                0 selects the default */
+    int sor_depth;           /* SOR kernels: 0 (default) colour-split sweeps;
+                                -2 colour-split, two FP32 correction
+                                iterations per HBM pass (temporal blocking);
+                                -1 natural-layout per-colour sweeps; >= 1
+                                natural-layout wavefront passes of that many
+                                iterations */
     int warm_start;          /* HC_WARM_* */
     int device;              /* CUDA device ordinal */
     int gravity_only;        /* 1: Poisson solver only (no hydro state); allows

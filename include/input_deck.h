@@ -135,7 +135,7 @@ typedef struct {
     int max_steps;              /* max_steps: stop after this many steps (0 = no cap) */
     int log_every;              /* log_every  (default 10, the reference's cadence) */
     double log_noise;           /* log_normal_noise: sigma of exp(sigma N(0,1)) on rho */
-    int sor_depth;              /* sor_depth: SOR iterations per HBM pass (0 = default) */
+    int sor_depth;              /* sor_depth: SOR kernels, as hc_config.sor_depth (0 = default) */
 } InputDeck;
 
 InputDeck *input_deck_create(const char *filename);
