@@ -86,9 +86,11 @@ cudaError_t conv3(const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *b
             attr_dev = dev;
         }
         const int tk = (d.nz + HT_K - 1) / HT_K, tj = (d.ny + HT_J - 1) / HT_J;
-        // about 6 CTAs per SM; at least 4 planes per CTA
+        // 6 CTAs per SM (shared-memory limit): as many plane chunks as fit one
+        // wave (rounding up would leave a second, nearly empty wave); at least
+        // 4 planes per CTA
         const long long want = 148LL * 6;
-        int chunks = (int)std::max(1LL, std::min((long long)(d.nx + 3) / 4, (want + tk * tj - 1) / ((long long)tk * tj)));
+        int chunks = (int)std::max(1LL, std::min((long long)(d.nx + 3) / 4, want / ((long long)tk * tj)));
         const int chunk = (d.nx + chunks - 1) / chunks;
         chunks = (d.nx + chunk - 1) / chunk;
         conv3_halo_kernel<<<dim3(tk, tj, chunks), 128, sizeof(HaloSmem), s>>>(tm, w, bias, out, d, out_mode, act,
