@@ -528,7 +528,8 @@ int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e
     if (e_out) {
         if (!u->have_weights) return HC_ERR_STATE;
         if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
-        out_up_kernel<<<a.g.nx * a.g.ny, 128, 0, s>>>(u->out0, u->L[0], u->scal, u->kscale, sp, e_out);
+        out_up_kernel<<<(unsigned)(((long long)a.g.nx * a.g.ny + OUT_UP_ROWS - 1) / OUT_UP_ROWS), 128, 0, s>>>(
+            u->out0, u->L[0], u->scal, u->kscale, sp, e_out);
     }
     return cudaGetLastError() == cudaSuccess ? HC_OK : HC_ERR_CUDA;
 }

@@ -264,42 +264,47 @@ __device__ __forceinline__ void lin_coarse(int i, int n0, int &a, int &b, float 
 }
 
 // e (colour-split FP32, whole grid) = trilinear upsample of the network output
-// times rms * kscale; zero on boundary cells.  One CTA per (i, j) row: the
-// row's coarse rows and weights in i and j are fixed, and thread m writes the
-// cells k = 2m and 2m+1 (one of each colour; consecutive m are consecutive in
-// each colour array).
+// times rms * kscale; zero on boundary cells.  A CTA takes OUT_UP_ROWS
+// consecutive (i, j) rows; per row the coarse rows and weights in i and j are
+// fixed, and thread m writes the cells k = 2m and 2m+1 (one of each colour;
+// consecutive m are consecutive in each colour array).
+constexpr int OUT_UP_ROWS = 16;
 __global__ void out_up_kernel(const float *__restrict__ out0, Dims d0, const double *__restrict__ sumsq, float kscale,
                               Split sp, float *__restrict__ e)
 {
-    const int row = blockIdx.x;   // i * ny + j
-    const int i = row / sp.ny, j = row - (row / sp.ny) * sp.ny;
     const double ms = *sumsq / (double)d0.n;
     const float sc = (float)sqrt(ms) * kscale;
-    const bool rin = i >= 1 && i <= sp.nx - 2 && j >= 1 && j <= sp.ny - 2;
-    int ia, ib, ja, jb;
-    float wi, wj;
-    lin_coarse(i, d0.nx, ia, ib, wi);
-    lin_coarse(j, d0.ny, ja, jb, wj);
-    const float *p00 = out0 + vidx(d0, ia, ja, 0), *p01 = out0 + vidx(d0, ia, jb, 0);
-    const float *p10 = out0 + vidx(d0, ib, ja, 0), *p11 = out0 + vidx(d0, ib, jb, 0);
-    for (int m = threadIdx.x; m < sp.H; m += blockDim.x) {
+    const long long rows = (long long)sp.nx * sp.ny;
+    for (int q = 0; q < OUT_UP_ROWS; q++) {
+        const long long row = (long long)blockIdx.x * OUT_UP_ROWS + q;   // i * ny + j
+        if (row >= rows) break;
+        const int i = (int)(row / sp.ny), j = (int)(row - (long long)i * sp.ny);
+        const bool rin = i >= 1 && i <= sp.nx - 2 && j >= 1 && j <= sp.ny - 2;
+        int ia, ib, ja, jb;
+        float wi, wj;
+        lin_coarse(i, d0.nx, ia, ib, wi);
+        lin_coarse(j, d0.ny, ja, jb, wj);
+        const float *p00 = out0 + vidx(d0, ia, ja, 0), *p01 = out0 + vidx(d0, ia, jb, 0);
+        const float *p10 = out0 + vidx(d0, ib, ja, 0), *p11 = out0 + vidx(d0, ib, jb, 0);
+        for (int m = threadIdx.x; m < sp.H; m += blockDim.x) {
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int k = 2 * m + h;
-            if (k >= sp.nz) break;
-            float val = 0.f;
-            if (rin && k >= 1 && k <= sp.nz - 2) {
-                int ka, kb;
-                float wk;
-                lin_coarse(k, d0.nz, ka, kb, wk);
-                const float c00 = p00[ka] * (1.f - wk) + p00[kb] * wk;
-                const float c01 = p01[ka] * (1.f - wk) + p01[kb] * wk;
-                const float c10 = p10[ka] * (1.f - wk) + p10[kb] * wk;
-                const float c11 = p11[ka] * (1.f - wk) + p11[kb] * wk;
-                const float c0 = c00 * (1.f - wj) + c01 * wj, c1 = c10 * (1.f - wj) + c11 * wj;
-                val = (c0 * (1.f - wi) + c1 * wi) * sc;
+            for (int h = 0; h < 2; h++) {
+                const int k = 2 * m + h;
+                if (k >= sp.nz) break;
+                float val = 0.f;
+                if (rin && k >= 1 && k <= sp.nz - 2) {
+                    int ka, kb;
+                    float wk;
+                    lin_coarse(k, d0.nz, ka, kb, wk);
+                    const float c00 = p00[ka] * (1.f - wk) + p00[kb] * wk;
+                    const float c01 = p01[ka] * (1.f - wk) + p01[kb] * wk;
+                    const float c10 = p10[ka] * (1.f - wk) + p10[kb] * wk;
+                    const float c11 = p11[ka] * (1.f - wk) + p11[kb] * wk;
+                    const float c0 = c00 * (1.f - wj) + c01 * wj, c1 = c10 * (1.f - wj) + c11 * wj;
+                    val = (c0 * (1.f - wi) + c1 * wi) * sc;
+                }
+                e[sp.at(i, j, k)] = val;
             }
-            e[sp.at(i, j, k)] = val;
         }
     }
 }
