@@ -19,6 +19,10 @@
 
 #include "hc_internal.cuh"
 
+#ifndef HC_CYCLE_REDUCTION
+#define HC_CYCLE_REDUCTION 1.0e-4   // residual reduction a correction cycle's sweeps aim for
+#endif
+
 using namespace hc;
 
 // ---------------------------------------------------------------- errors
@@ -760,7 +764,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         // grid's condition number on a cold start.  In the last cycle the
         // sweeps run to the reference's own test: a red-black sweep whose
         // update norm max |phi_GS - phi_old| is below tol.
-        const double thresh = std::max(a.tol, 1.0e-4 * dmax);
+        const double thresh = std::max(a.tol, HC_CYCLE_REDUCTION * dmax);
         const int budget = a.max_iter - total;
         CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));
         CK(grav_reset_slots(a, 0, budget + 8, c->s));

@@ -18,6 +18,10 @@
 #include "sor_split.cuh"
 #include "sor_wave_split.cuh"
 
+#ifndef HC_MIXED_PAIR
+#define HC_MIXED_PAIR 1   // pair forms of the FP64 residual / update where the layout allows
+#endif
+
 namespace hc {
 
 int lmax_ncoef(int lmax) { return (lmax + 1) * (lmax + 1); }
@@ -528,6 +532,94 @@ __global__ void __launch_bounds__(256) mixed_update_kernel(GravArgs a, const flo
     if (threadIdx.x == 0 && b > 0.0) atomic_max_nonneg(&a.sc->resid_bits, b);
 }
 
+// Pair forms of the residual and the update for the colour-split layout with
+// even nz: thread m of a row takes the cells k = 2m and 2m+1 -- one of each
+// colour, both at index m of their colour array -- so phi moves as 16-byte
+// pairs and each colour array is written with unit stride.  Per cell the
+// arithmetic is that of mixed_residual_kernel / mixed_update_kernel.
+constexpr int PAIR_NT = 128;
+__global__ void __launch_bounds__(PAIR_NT) mixed_residual_pair_kernel(GravArgs a, float *r32, float *e32, Split sp)
+{
+    const Geom g = a.g;
+    const MixConst mc = mix_const(a);
+    const double ifac = 1.0 / mc.fac;
+    const long long sI = (long long)g.ny * g.nz, sJ = g.nz;
+    const long long rows = (long long)g.nx * g.ny;
+    const double *phi = a.phi;
+    double mx = 0.0;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int i = (int)(row / g.ny), j = (int)(row % g.ny);
+        const bool inner = i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2;
+        const long long c0 = row * sJ;
+        const int cc = (i + j) & 1;   // colour of k = 2m
+        float *r0 = r32 + cc * sp.cs + row * sp.H, *r1 = r32 + (cc ^ 1) * sp.cs + row * sp.H;
+        float *e0 = e32 + cc * sp.cs + row * sp.H, *e1 = e32 + (cc ^ 1) * sp.cs + row * sp.H;
+        for (int m = threadIdx.x; m < sp.H; m += PAIR_NT) {
+            const long long c = c0 + 2 * m;
+            float d[2] = { 0.f, 0.f };
+            if (inner) {
+                const double2 pc = *reinterpret_cast<const double2 *>(phi + c);
+                const double2 xm = *reinterpret_cast<const double2 *>(phi + c - sI);
+                const double2 xp = *reinterpret_cast<const double2 *>(phi + c + sI);
+                const double2 ym = *reinterpret_cast<const double2 *>(phi + c - sJ);
+                const double2 yp = *reinterpret_cast<const double2 *>(phi + c + sJ);
+                const double zl = m > 0 ? phi[c - 1] : 0.0, zr = 2 * m + 2 < g.nz ? phi[c + 2] : 0.0;
+                double r0v, r1v;
+                if (a.rho) {
+                    const double2 rr = *reinterpret_cast<const double2 *>(a.rho + c);
+                    r0v = rr.x;
+                    r1v = rr.y;
+                } else {
+                    const float2 rr = *reinterpret_cast<const float2 *>(a.rho32 + c);
+                    r0v = (double)rr.x;
+                    r1v = (double)rr.y;
+                }
+                const int k = 2 * m;
+                if (k >= 1 && k <= g.nz - 2) {
+                    const double lap = (xm.x + xp.x) * mc.ix2 + (ym.x + yp.x) * mc.iy2 + (zl + pc.y) * mc.iz2;
+                    const double dd = (lap - mc.fpg * r0v) * ifac - pc.x;
+                    mx = tmax(mx, fabs(dd));
+                    d[0] = (float)dd;
+                }
+                if (k + 1 >= 1 && k + 1 <= g.nz - 2) {
+                    const double lap = (xm.y + xp.y) * mc.ix2 + (ym.y + yp.y) * mc.iy2 + (pc.x + zr) * mc.iz2;
+                    const double dd = (lap - mc.fpg * r1v) * ifac - pc.y;
+                    mx = tmax(mx, fabs(dd));
+                    d[1] = (float)dd;
+                }
+            }
+            r0[m] = d[0];
+            r1[m] = d[1];
+            e0[m] = 0.f;
+            e1[m] = 0.f;
+        }
+    }
+    const double b = block_max_any<PAIR_NT>(mx);
+    if (threadIdx.x == 0) atomic_max_nonneg((unsigned long long *)&a.sc->resnorm, b);
+}
+
+__global__ void __launch_bounds__(PAIR_NT) mixed_update_pair_kernel(GravArgs a, const float *e32, Split sp, float sign)
+{
+    const long long rows = (long long)a.g.nx * a.g.ny;
+    float mx = 0.f;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int i = (int)(row / a.g.ny), j = (int)(row % a.g.ny);
+        const int cc = (i + j) & 1;
+        const float *f0 = e32 + cc * sp.cs + row * sp.H, *f1 = e32 + (cc ^ 1) * sp.cs + row * sp.H;
+        double *prow = a.phi + row * a.g.nz;
+        for (int m = threadIdx.x; m < sp.H; m += PAIR_NT) {
+            const float ea = sign * f0[m], eb = sign * f1[m];
+            double2 p = *reinterpret_cast<const double2 *>(prow + 2 * m);
+            p.x += (double)ea;
+            p.y += (double)eb;
+            *reinterpret_cast<double2 *>(prow + 2 * m) = p;
+            mx = tmax(mx, tmax(fabsf(ea), fabsf(eb)));
+        }
+    }
+    const double b = block_max_any<PAIR_NT>((double)mx);
+    if (threadIdx.x == 0 && b > 0.0) atomic_max_nonneg(&a.sc->resid_bits, b);
+}
+
 constexpr int S32_BX = 32, S32_BY = 8;
 
 __global__ void __launch_bounds__(S32_BX * S32_BY)
@@ -579,15 +671,28 @@ static Split split_or_natural(const GravArgs &a, bool split)
     return sp;
 }
 
+// the pair kernels need the colour-split layout, even nz and 16-byte aligned rows
+static bool pair_ok(const GravArgs &a, bool split)
+{
+    return HC_MIXED_PAIR && split && a.g.nz % 2 == 0 && ((uintptr_t)a.phi % 16) == 0 &&
+           ((uintptr_t)(a.rho ? (const void *)a.rho : (const void *)a.rho32) % 16) == 0;
+}
+
 cudaError_t mixed_residual(const GravArgs &a, float *r32, float *e32, bool split, cudaStream_t s)
 {
-    mixed_residual_kernel<<<148 * 16, 256, 0, s>>>(a, r32, e32, split_or_natural(a, split));
+    if (pair_ok(a, split))
+        mixed_residual_pair_kernel<<<148 * 32, PAIR_NT, 0, s>>>(a, r32, e32, make_split(a.g));
+    else
+        mixed_residual_kernel<<<148 * 16, 256, 0, s>>>(a, r32, e32, split_or_natural(a, split));
     return cudaGetLastError();
 }
 
 cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, float sign, cudaStream_t s)
 {
-    mixed_update_kernel<<<148 * 16, 256, 0, s>>>(a, e32, split_or_natural(a, split), sign);
+    if (pair_ok(a, split))
+        mixed_update_pair_kernel<<<148 * 32, PAIR_NT, 0, s>>>(a, e32, make_split(a.g), sign);
+    else
+        mixed_update_kernel<<<148 * 16, 256, 0, s>>>(a, e32, split_or_natural(a, split), sign);
     return cudaGetLastError();
 }
 
