@@ -74,7 +74,10 @@ inline Split make_split(const Geom &g)
     return s;
 }
 
-constexpr int SPLIT_BX = 32, SPLIT_BY = 8;
+#ifndef HC_SPLIT_BY
+#define HC_SPLIT_BY 8
+#endif
+constexpr int SPLIT_BX = 32, SPLIT_BY = HC_SPLIT_BY;   // rows of a CTA
 
 // Programmatic dependent launch: a sweep launched with programmatic stream
 // serialisation may be scheduled while the previous sweep's last CTAs still
