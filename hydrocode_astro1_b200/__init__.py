@@ -107,6 +107,9 @@ CAPI = {
     "hc_set_unet_passes": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_cycles": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_record_cycle": (C.c_int, [C.c_void_p, C.c_int]),
+    "hc_checkpoint_save": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_longlong]),
+    "hc_checkpoint_wait": (C.c_int, [C.c_void_p]),
+    "hc_checkpoint_load": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "hc_unet_train": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint, C.POINTER(C.c_double)]),
     "hc_unet_loss_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
                                     C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float),
@@ -350,6 +353,22 @@ class HydroSolver3D:
     def unet_cycles(self, n):
         """Correction cycles that start from the network's prediction (default 2)."""
         _check(self.L.hc_set_unet_cycles(self.h, int(n)), "hc_set_unet_cycles")
+
+    def checkpoint_save(self, path, t=0.0, step=0):
+        """Pack the state (and potentials) on the device and write `path` in
+        the background; the solver may keep stepping.  checkpoint_wait()
+        returns when the file is complete."""
+        _check(self.L.hc_checkpoint_save(self.h, os.fsencode(path), float(t), int(step)), "hc_checkpoint_save")
+
+    def checkpoint_wait(self):
+        _check(self.L.hc_checkpoint_wait(self.h), "hc_checkpoint_wait")
+
+    def checkpoint_load(self, path):
+        """Restore a checkpoint written by checkpoint_save; returns (t, step)."""
+        t = C.c_double(0.0)
+        n = C.c_longlong(0)
+        _check(self.L.hc_checkpoint_load(self.h, os.fsencode(path), C.byref(t), C.byref(n)), "hc_checkpoint_load")
+        return t.value, n.value
 
     def unet_record_cycle(self, c):
         """With collection on: the correction cycle whose residual is recorded."""

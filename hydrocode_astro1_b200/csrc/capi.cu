@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "hc_internal.cuh"
@@ -106,6 +108,15 @@ struct hc_ctx {
     int unet_passes;             // learned-start predictions per solve (>= 1)
     int unet_cycles;             // correction cycles that start from a prediction (0: 2)
     int unet_record_cycle;       // the cycle whose residual is recorded for training (0: 1)
+    // checkpoints: device packing buffer, copy stream, writer thread
+    unsigned char *ck_dev;
+    size_t ck_dev_bytes;
+    unsigned char *ck_host[2];   // pinned chunks
+    cudaStream_t ck_stream;
+    cudaEvent_t ck_ev[3];
+    std::thread *ck_thread;
+    int ck_status;
+    char ck_err[256];
 };
 
 static cudaEvent_t ev_get(hc_ctx *c)
@@ -208,6 +219,16 @@ static void free_ctx(hc_ctx *c)
     for (auto e : c->evpool) cudaEventDestroy(e);
     if (c->t0) cudaEventDestroy(c->t0);
     if (c->t1) cudaEventDestroy(c->t1);
+    if (c->ck_thread) {
+        c->ck_thread->join();
+        delete c->ck_thread;
+    }
+    cudaFree(c->ck_dev);
+    for (int b = 0; b < 2; b++)
+        if (c->ck_host[b]) cudaFreeHost(c->ck_host[b]);
+    for (int e = 0; e < 3; e++)
+        if (c->ck_ev[e]) cudaEventDestroy(c->ck_ev[e]);
+    if (c->ck_stream) cudaStreamDestroy(c->ck_stream);
     if (c->s) cudaStreamDestroy(c->s);
     unet_destroy(c->unet);
     delete c;
@@ -1390,4 +1411,240 @@ extern "C" int hc_set_unet_record_cycle(hc_ctx *c, int cycle)
     if (!c || cycle < 1 || cycle > 8) return set_err(HC_ERR_ARG, "cycle must be 1..8");
     c->unet_record_cycle = cycle;
     return HC_OK;
+}
+
+// ---------------------------------------------------------------- checkpoints
+// Binary checkpoint of everything the next step reads: the conserved state
+// in the context's own precision (bit for bit), and with self-gravity the
+// potential (the next solve's starting iterate and boundary values) and the
+// potential of the last converged solve (g); plus the step parity.  The CFL
+// signal speed is recomputed from the state on load (a max: the same value).
+// File: CkptHeader, then the payload -- 5 state fields (nx*ny*nz words each,
+// k fastest), phi, phig -- with an FNV-1a 64 checksum of the payload in the
+// header.  Saving packs the payload into one device buffer on the compute
+// stream (device to device), then a writer thread copies it to the host on
+// its own stream through two pinned 64 MB chunks and writes the file while
+// the context keeps stepping.
+namespace {
+struct CkptHeader {
+    char magic[8];      // "HCCKPT01"
+    int32_t version, header_bytes;
+    int32_t nx, ny, nz, precision, gravity, parity;
+    int64_t step;
+    double t, lo[3], hi[3], gamma, G;
+    uint64_t payload_bytes, checksum;
+};
+constexpr size_t CK_CHUNK = (size_t)64 << 20;
+
+uint64_t fnv1a(uint64_t h, const unsigned char *p, size_t n)
+{
+    for (size_t i = 0; i < n; i++) {
+        h ^= p[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+constexpr uint64_t FNV_OFFSET = 14695981039346656037ULL;
+
+size_t ck_payload_bytes(const hc_ctx *c)
+{
+    const size_t n = (size_t)c->g.n;
+    return 5 * n * (c->cfg.precision == HC_FP64 ? 8 : 4) + (c->gravity ? 2 * n * 8 : 0);
+}
+
+void ck_fill_header(const hc_ctx *c, CkptHeader &h)
+{
+    memset(&h, 0, sizeof h);
+    memcpy(h.magic, "HCCKPT01", 8);
+    h.version = 1;
+    h.header_bytes = (int32_t)sizeof(CkptHeader);
+    h.nx = c->g.nx;
+    h.ny = c->g.ny;
+    h.nz = c->g.nz;
+    h.precision = c->cfg.precision;
+    h.gravity = c->gravity;
+    h.parity = c->parity;
+    h.lo[0] = c->cfg.xmin; h.lo[1] = c->cfg.ymin; h.lo[2] = c->cfg.zmin;
+    h.hi[0] = c->cfg.xmax; h.hi[1] = c->cfg.ymax; h.hi[2] = c->cfg.zmax;
+    h.gamma = c->cfg.gamma;
+    h.G = c->cfg.G;
+    h.payload_bytes = ck_payload_bytes(c);
+}
+
+int ck_buffers(hc_ctx *c, size_t bytes)
+{
+    if (!c->ck_dev || c->ck_dev_bytes < bytes) {
+        cudaFree(c->ck_dev);
+        c->ck_dev = nullptr;
+        c->ck_dev_bytes = 0;
+        if (dmalloc((void **)&c->ck_dev, bytes)) return set_err(HC_ERR_NOMEM, "checkpoint packing buffer");
+        c->ck_dev_bytes = bytes;
+    }
+    for (int b = 0; b < 2; b++)
+        if (!c->ck_host[b] && cudaMallocHost((void **)&c->ck_host[b], CK_CHUNK) != cudaSuccess)
+            return set_err(HC_ERR_NOMEM, "pinned checkpoint chunks");
+    if (!c->ck_stream && cudaStreamCreateWithFlags(&c->ck_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return set_err(HC_ERR_CUDA, "checkpoint stream");
+    for (int e = 0; e < 3; e++)
+        if (!c->ck_ev[e] && cudaEventCreateWithFlags(&c->ck_ev[e], cudaEventDisableTiming) != cudaSuccess)
+            return set_err(HC_ERR_CUDA, "checkpoint events");
+    return HC_OK;
+}
+
+// writer thread: chunk k is copied into pinned buffer k % 2 while chunk k-1
+// is hashed and written
+void ck_writer(hc_ctx *c, std::string path, CkptHeader h)
+{
+    auto fail = [&](int code, const char *what) {
+        c->ck_status = code;
+        snprintf(c->ck_err, sizeof c->ck_err, "checkpoint %s: %s", path.c_str(), what);
+    };
+    if (cudaSetDevice(c->dev) != cudaSuccess) return fail(HC_ERR_CUDA, "cudaSetDevice");
+    FILE *f = fopen(path.c_str(), "wb");
+    if (!f) return fail(HC_ERR_ARG, "cannot open for writing");
+    bool ok = fwrite(&h, sizeof h, 1, f) == 1;
+    const size_t bytes = h.payload_bytes;
+    const size_t nch = (bytes + CK_CHUNK - 1) / CK_CHUNK;
+    uint64_t hash = FNV_OFFSET;
+    for (size_t k = 0; ok && k <= nch; k++) {
+        if (k < nch) {
+            const size_t off = k * CK_CHUNK, len = std::min(CK_CHUNK, bytes - off);
+            if (cudaMemcpyAsync(c->ck_host[k & 1], c->ck_dev + off, len, cudaMemcpyDeviceToHost, c->ck_stream) !=
+                    cudaSuccess ||
+                cudaEventRecord(c->ck_ev[k & 1], c->ck_stream) != cudaSuccess) {
+                fclose(f);
+                return fail(HC_ERR_CUDA, "device-to-host copy");
+            }
+        }
+        if (k >= 1) {
+            const size_t q = k - 1, off = q * CK_CHUNK, len = std::min(CK_CHUNK, bytes - off);
+            if (cudaEventSynchronize(c->ck_ev[q & 1]) != cudaSuccess) {
+                fclose(f);
+                return fail(HC_ERR_CUDA, "device-to-host copy");
+            }
+            hash = fnv1a(hash, c->ck_host[q & 1], len);
+            ok = fwrite(c->ck_host[q & 1], 1, len, f) == len;
+        }
+    }
+    h.checksum = hash;
+    ok = ok && fseek(f, 0, SEEK_SET) == 0 && fwrite(&h, sizeof h, 1, f) == 1;
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) fail(HC_ERR_ARG, "write failed");
+}
+}  // namespace
+
+extern "C" int hc_checkpoint_wait(hc_ctx *c)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null argument");
+    if (c->ck_thread) {
+        c->ck_thread->join();
+        delete c->ck_thread;
+        c->ck_thread = nullptr;
+    }
+    const int st = c->ck_status;
+    c->ck_status = HC_OK;
+    if (st) return set_err(st, c->ck_err);
+    return HC_OK;
+}
+
+extern "C" int hc_checkpoint_save(hc_ctx *c, const char *path, double t, long long step)
+{
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    if (!c || !path) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = hc_checkpoint_wait(c);   // one write in flight per context
+    if (rc) return rc;
+    const size_t n = (size_t)c->g.n, bytes = ck_payload_bytes(c);
+    rc = ck_buffers(c, bytes);
+    if (rc) return rc;
+    const bool f64 = c->cfg.precision == HC_FP64;
+    const size_t w = f64 ? 8 : 4;
+    for (int v = 0; v < 5; v++) {
+        const void *src = f64 ? (const void *)c->q64[c->cur][v] : (const void *)c->q32[c->cur][v];
+        CK(cudaMemcpyAsync(c->ck_dev + v * n * w, src, n * w, cudaMemcpyDeviceToDevice, c->s));
+    }
+    if (c->gravity) {
+        CK(cudaMemcpyAsync(c->ck_dev + 5 * n * w, c->phi, n * 8, cudaMemcpyDeviceToDevice, c->s));
+        CK(cudaMemcpyAsync(c->ck_dev + 5 * n * w + n * 8, c->phig, n * 8, cudaMemcpyDeviceToDevice, c->s));
+    }
+    CK(cudaEventRecord(c->ck_ev[2], c->s));
+    CK(cudaStreamWaitEvent(c->ck_stream, c->ck_ev[2], 0));
+    CkptHeader h;
+    ck_fill_header(c, h);
+    h.t = t;
+    h.step = step;
+    c->ck_status = HC_OK;
+    try {
+        c->ck_thread = new std::thread(ck_writer, c, std::string(path), h);
+    } catch (...) {
+        return set_err(HC_ERR_STATE, "cannot start the checkpoint writer thread");
+    }
+    return HC_OK;
+}
+
+extern "C" int hc_checkpoint_load(hc_ctx *c, const char *path, double *t, long long *step)
+{
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    if (!c || !path) return set_err(HC_ERR_ARG, "null argument");
+    CK(cudaSetDevice(c->dev));
+    int rc = hc_checkpoint_wait(c);
+    if (rc) return rc;
+    FILE *f = fopen(path, "rb");
+    if (!f) return set_err(HC_ERR_ARG, "checkpoint: cannot open file");
+    CkptHeader h, want;
+    ck_fill_header(c, want);
+    auto bad = [&](const char *what) {
+        fclose(f);
+        return set_err(HC_ERR_ARG, what);
+    };
+    if (fread(&h, sizeof h, 1, f) != 1 || memcmp(h.magic, "HCCKPT01", 8) != 0 || h.version != 1 ||
+        h.header_bytes != (int32_t)sizeof(CkptHeader))
+        return bad("checkpoint: not a version-1 checkpoint file");
+    if (h.nx != want.nx || h.ny != want.ny || h.nz != want.nz || h.precision != want.precision ||
+        h.gravity != want.gravity || h.payload_bytes != want.payload_bytes)
+        return bad("checkpoint: grid, precision or gravity differ from this context");
+    for (int a = 0; a < 3; a++)
+        if (h.lo[a] != want.lo[a] || h.hi[a] != want.hi[a]) return bad("checkpoint: domain differs from this context");
+    if (h.gamma != want.gamma || h.G != want.G) return bad("checkpoint: gamma or G differ from this context");
+    const size_t bytes = h.payload_bytes;
+    rc = ck_buffers(c, bytes);
+    if (rc) {
+        fclose(f);
+        return rc;
+    }
+    // whole payload into the packing buffer first: a short or corrupt file
+    // leaves the context's state untouched
+    uint64_t hash = FNV_OFFSET;
+    const size_t nch = (bytes + CK_CHUNK - 1) / CK_CHUNK;
+    for (size_t k = 0; k < nch; k++) {
+        const size_t off = k * CK_CHUNK, len = std::min(CK_CHUNK, bytes - off);
+        unsigned char *buf = c->ck_host[k & 1];
+        if (k >= 2) CK(cudaEventSynchronize(c->ck_ev[k & 1]));   // the copy out of this buffer is done
+        if (fread(buf, 1, len, f) != len) {
+            cudaStreamSynchronize(c->ck_stream);
+            return bad("checkpoint: file is shorter than its header says");
+        }
+        hash = fnv1a(hash, buf, len);
+        CK(cudaMemcpyAsync(c->ck_dev + off, buf, len, cudaMemcpyHostToDevice, c->ck_stream));
+        CK(cudaEventRecord(c->ck_ev[k & 1], c->ck_stream));
+    }
+    fclose(f);
+    CK(cudaStreamSynchronize(c->ck_stream));
+    if (hash != h.checksum) return set_err(HC_ERR_ARG, "checkpoint: payload checksum mismatch");
+    const size_t n = (size_t)c->g.n;
+    const bool f64 = c->cfg.precision == HC_FP64;
+    const size_t w = f64 ? 8 : 4;
+    for (int v = 0; v < 5; v++) {
+        void *dst = f64 ? (void *)c->q64[c->cur][v] : (void *)c->q32[c->cur][v];
+        CK(cudaMemcpyAsync(dst, c->ck_dev + v * n * w, n * w, cudaMemcpyDeviceToDevice, c->s));
+    }
+    if (c->gravity) {
+        CK(cudaMemcpyAsync(c->phi, c->ck_dev + 5 * n * w, n * 8, cudaMemcpyDeviceToDevice, c->s));
+        CK(cudaMemcpyAsync(c->phig, c->ck_dev + 5 * n * w + n * 8, n * 8, cudaMemcpyDeviceToDevice, c->s));
+    }
+    c->parity = h.parity;
+    c->cfl_valid = 0;
+    if (t) *t = h.t;
+    if (step) *step = h.step;
+    return sync_ctx(c);
 }

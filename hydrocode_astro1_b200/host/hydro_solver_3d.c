@@ -101,6 +101,8 @@ GodunovHLLC3D *solver3d_create_from_deck(const InputDeck *d)   /* hydro_solver_3
     s->max_steps = d->max_steps;
     s->log_every = d->log_every > 0 ? d->log_every : 10;
     strncpy(s->unet_weights, d->unet_weights, sizeof s->unet_weights - 1);
+    s->checkpoint_every = d->checkpoint_every;
+    strncpy(s->checkpoint_file, d->checkpoint_file, sizeof s->checkpoint_file - 1);
     if (s->gravity_solver) {
         gravity_set_solver_params(s->gravity_solver, d->grav_omega, d->grav_max_iter, d->grav_tolerance);
         s->gravity_solver->lmax = d->grav_lmax;
@@ -220,6 +222,36 @@ int solver3d_step(GodunovHLLC3D *s, int nsteps)
     return worst;
 }
 
+/* ---------------------------------------------------------------- checkpoints */
+int solver3d_write_checkpoint(GodunovHLLC3D *s, const char *path, double t, long long step)
+{
+    if (upload_if_dirty(s)) return -1;
+    if (hc_checkpoint_save(s->dev, path, t, step) != HC_OK) {
+        fprintf(stderr, "Error: checkpoint %s: %s\n", path, hc_last_error());
+        return -1;
+    }
+    return 0;
+}
+
+int solver3d_read_checkpoint(GodunovHLLC3D *s, const char *path, double *t, long long *step)
+{
+    if (ensure_device(s)) return -1;
+    double tt = 0.0;
+    long long st = 0;
+    if (hc_checkpoint_load(s->dev, path, &tt, &st) != HC_OK) {
+        fprintf(stderr, "Error: %s\n", hc_last_error());
+        return -1;
+    }
+    s->host_dirty = 0;     /* the device state is the restored one */
+    s->device_dirty = 1;
+    s->ck_restored = 1;
+    s->ck_t = tt;
+    s->steps_taken = st;
+    if (t) *t = tt;
+    if (step) *step = st;
+    return 0;
+}
+
 /* ---------------------------------------------------------------- ICs */
 void set_initial_conditions_3d(GodunovHLLC3D *s, ProblemType problem)
 {
@@ -307,6 +339,19 @@ void write_output_vtk(const GodunovHLLC3D *solver, int step)   /* :2376-2435 */
 /* ---------------------------------------------------------------- restart */
 int load_from_csv_restart(GodunovHLLC3D *s, const char *filename)   /* :2139-2235 */
 {
+    {   /* a binary checkpoint of this library: exact restart */
+        FILE *b = fopen(filename, "rb");
+        char magic[8] = { 0 };
+        const int bin = b && fread(magic, 1, 8, b) == 8 && memcmp(magic, "HCCKPT01", 8) == 0;
+        if (b) fclose(b);
+        if (bin) {
+            double t = 0.0;
+            long long st = 0;
+            if (solver3d_read_checkpoint(s, filename, &t, &st)) return -1;
+            printf("Loaded binary checkpoint %s (t = %.17g, step %lld)\n", filename, t, st);
+            return 0;
+        }
+    }
     FILE *fp = fopen(filename, "r");
     if (!fp) {
         fprintf(stderr, "Error: Could not open restart file '%s'\n", filename);
@@ -384,8 +429,12 @@ static void run_loop(GodunovHLLC3D *s, double t, double t_end, double output_dt,
         }
         if (step_counter % s->log_every == 0)
             printf("Step %d, t = %.5f, dt = %.5e\n", step_counter, t, s->dt);
+        if (s->checkpoint_every > 0 && step_counter % s->checkpoint_every == 0)
+            solver3d_write_checkpoint(s, s->checkpoint_file, t, s->steps_taken);   /* written in the background */
         if (s->max_steps > 0 && step_counter >= s->max_steps) break;
     }
+    if (s->dev && hc_checkpoint_wait(s->dev) != HC_OK)
+        fprintf(stderr, "Error: checkpoint %s: %s\n", s->checkpoint_file, hc_last_error());
     if (t - (next_output_time - output_dt) > 1e-6) {
         write_output_to_file_3d(s, output_count);
         write_output_vtk(s, output_count);
@@ -405,6 +454,11 @@ void run_simulation_3d(GodunovHLLC3D *s, double t_end, double output_dt)   /* :2
 void run_simulation_3d_restart(GodunovHLLC3D *s, double t_start, double t_end, double output_dt,
                                int start_output_count)   /* :2286-2330 */
 {
+    if (s->ck_restored && s->ck_t != t_start) {
+        printf("Binary checkpoint: starting from its stored time t = %.17g (restart_time %.5f ignored)\n", s->ck_t,
+               t_start);
+        t_start = s->ck_t;
+    }
     printf("Restarting 3D simulation from t=%.5f to t=%.5f\n", t_start, t_end);
     printf("Starting output count: %d\n", start_output_count);
     printf("Grid: %d x %d x %d = %d cells\n", s->nx, s->ny, s->nz, s->nx * s->ny * s->nz);

@@ -123,6 +123,7 @@ static const Field FIELDS[] = {
     F("warm_start", K_WARM, warm_start), F("unet_weights", K_STR, unet_weights),
     F("max_steps", K_INT, max_steps), F("log_every", K_INT, log_every),
     F("log_normal_noise", K_DBL, log_noise), F("sor_depth", K_INT, sor_depth),
+    F("checkpoint_every", K_INT, checkpoint_every), F("checkpoint_file", K_STR, checkpoint_file),
 };
 
 static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
@@ -171,6 +172,7 @@ static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
     d->grav_tolerance = 1.0e-6;
     d->grav_max_iter = 10000;
     d->log_every = 10;
+    strcpy(d->checkpoint_file, "checkpoint.ckpt");
 }
 
 static int is_true(const char *v) { return strcmp(v, "true") == 0 || strcmp(v, "1") == 0; }

@@ -85,6 +85,10 @@ typedef struct GodunovHLLC3D {
     int log_every;
     char unet_weights[256];
     long long steps_taken;
+    int checkpoint_every;      /* binary checkpoint every N steps of a run (0 = off) */
+    char checkpoint_file[256];
+    int ck_restored;           /* a binary checkpoint was loaded: its time is ck_t */
+    double ck_t;
 } GodunovHLLC3D;
 
 GodunovHLLC3D *solver3d_create(int nx, int ny, int nz,
@@ -114,5 +118,13 @@ GodunovHLLC3D *solver3d_create_from_deck(const InputDeck *deck);
 int solver3d_step(GodunovHLLC3D *solver, int nsteps);
 /* Copy the device state into U (and gx/gy/gz, the gravity potential). */
 int solver3d_sync_host(GodunovHLLC3D *solver);
+/* Binary checkpoint (hc_checkpoint_save): exact state, potentials and step
+ * parity, with t and step; written in the background -- the next checkpoint,
+ * a read and solver3d_destroy wait for it.  Returns 0 or -1 (message on
+ * stderr).  load_from_csv_restart also accepts such a file (recognised by its
+ * magic), and run_simulation_3d_restart then starts from the stored time. */
+int solver3d_write_checkpoint(GodunovHLLC3D *solver, const char *path, double t, long long step);
+/* Restore a binary checkpoint; *t and *step (nullable) receive the stored values. */
+int solver3d_read_checkpoint(GodunovHLLC3D *solver, const char *path, double *t, long long *step);
 
 #endif /* HYDRO_SOLVER_3D_H */

@@ -225,6 +225,29 @@ int hc_set_unet_cycles(hc_ctx *ctx, int cycles);
  * residual is recorded as a training sample (1..8, default 1). */
 int hc_set_unet_record_cycle(hc_ctx *ctx, int cycle);
 
+/* Binary checkpoint and restart.  No counterpart in the reference, whose
+ * restart reads its own CSV output (hydro_solver_3d.c:2142-2351): 6 decimal
+ * digits per value, so a restarted run drifts from the uninterrupted one.
+ * hc_checkpoint_save packs, on the device, everything the next step reads
+ * -- the conserved state in the context's precision, and with self-gravity
+ * the potential (the next solve's starting iterate and boundary values) and
+ * the potential of the last converged solve (from which g is formed) -- and
+ * returns while a writer thread copies the packed buffer to the host on its
+ * own stream and writes `path`; the context may keep stepping meanwhile.  One
+ * write is in flight per context: the next save, a load, hc_checkpoint_wait
+ * and hc_destroy wait for it, and hc_checkpoint_wait returns its status.
+ * hc_checkpoint_load checks the header (grid, precision, gravity, domain,
+ * gamma, G) and a checksum of the payload before it replaces anything; a run
+ * restarted from it continues bit for bit as the uninterrupted run.  t and
+ * step are stored for the caller and returned by the load (each nullable).
+ * Layout: a 136-byte header (hydrocode_astro1_b200/checkpoint.py lists its
+ * fields; magic "HCCKPT01"), then 5 state fields of nx*ny*nz
+ * words (8 bytes for HC_FP64, 4 for HC_FP32; k fastest), then phi and the
+ * last converged phi (nx*ny*nz doubles each) when G > 0. */
+int hc_checkpoint_save(hc_ctx *ctx, const char *path, double t, long long step);
+int hc_checkpoint_wait(hc_ctx *ctx);
+int hc_checkpoint_load(hc_ctx *ctx, const char *path, double *t, long long *step);
+
 /* Diagnostics of the tensor-core convolution kernels (no reference
  * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16
  * channels (channels last), weights w[co][tap][ci] (16*27*16 BF16, tap =

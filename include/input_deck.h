@@ -136,6 +136,8 @@ typedef struct {
     int log_every;              /* log_every  (default 10, the reference's cadence) */
     double log_noise;           /* log_normal_noise: sigma of exp(sigma N(0,1)) on rho */
     int sor_depth;              /* sor_depth: SOR kernels, as hc_config.sor_depth (0 = default) */
+    int checkpoint_every;       /* checkpoint_every: binary checkpoint every N steps (0 = off) */
+    char checkpoint_file[256];  /* checkpoint_file (default checkpoint.ckpt; the latest one is kept) */
 } InputDeck;
 
 InputDeck *input_deck_create(const char *filename);
