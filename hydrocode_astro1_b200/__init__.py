@@ -45,6 +45,7 @@ class Config(C.Structure):
         ("grav_bc", C.c_int), ("lmax", C.c_int), ("omega", C.c_double),
         ("tol", C.c_double), ("max_iter", C.c_int), ("sor_depth", C.c_int),
         ("warm_start", C.c_int), ("device", C.c_int), ("gravity_only", C.c_int),
+        ("recon", C.c_int),
     ]
 
 

@@ -79,6 +79,7 @@ struct hc_ctx {
     // gravity
     double *phi, *phig, *rho_ext, *phi2;
     double *phs, *rhs;           // colour-split potential and density (FP64 solve)
+    double *plm;                 // MUSCL-Hancock face-state buffer (20 values per cell; recon = 1)
     float *e32, *r32, *e32b;     // mixed precision correction (ping-pong) / residual
     double *gx, *gy, *gz;
     double *res;
@@ -207,7 +208,7 @@ static void free_ctx(hc_ctx *c)
             if (c->q32[b][v] && v == 0) cudaFree(c->q32[b][0]);
         }
     cudaFree(c->phi); cudaFree(c->phig); cudaFree(c->rho_ext); cudaFree(c->phi2);
-    cudaFree(c->phs); cudaFree(c->rhs);
+    cudaFree(c->phs); cudaFree(c->rhs); cudaFree(c->plm);
     cudaFree(c->e32); cudaFree(c->r32); cudaFree(c->e32b);
     cudaFree(c->gx); cudaFree(c->gy); cudaFree(c->gz);
     cudaFree(c->res); cudaFree(c->scratch); cudaFree(c->mom);
@@ -276,6 +277,14 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
     }
     if (k.lmax < 0 || k.lmax > 12) {
         set_err(HC_ERR_ARG, "lmax %d outside 0..12", k.lmax);
+        return nullptr;
+    }
+    if (k.recon != 0 && k.recon != 1) {
+        set_err(HC_ERR_ARG, "unknown reconstruction %d (0 piecewise constant, 1 MUSCL-Hancock)", k.recon);
+        return nullptr;
+    }
+    if (k.recon == 1 && k.precision != HC_FP64) {
+        set_err(HC_ERR_ARG, "MUSCL-Hancock reconstruction runs in HC_FP64 only");
         return nullptr;
     }
     if (!(k.xmax > k.xmin) || !(k.ymax > k.ymin) || !(k.zmax > k.zmin)) {
@@ -1123,7 +1132,14 @@ static int step_once(hc_ctx *c, int *grav_status)
     }
     {
         FamTimer t(c, FAM_HYDRO);
-        CK(f64 ? fp64_interior(a, interior_chunks(c), c->s) : fp32_interior(a, interior_chunks(c), c->s));
+        if (f64 && c->cfg.recon == 1) {
+            if (!c->plm && dmalloc((void **)&c->plm, 20 * (size_t)c->g.n * sizeof(double)))
+                return set_err(HC_ERR_NOMEM, "MUSCL-Hancock face-state buffer");
+            CK(fp64_plm_interior(a, c->plm, c->s));
+            c->launches += 1;
+        } else {
+            CK(f64 ? fp64_interior(a, interior_chunks(c), c->s) : fp32_interior(a, interior_chunks(c), c->s));
+        }
     }
     {
         FamTimer t(c, FAM_BC);

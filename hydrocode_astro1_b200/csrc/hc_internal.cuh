@@ -102,6 +102,8 @@ cudaError_t fp64_bc(const HydroArgs &a, int axis, cudaStream_t s);
 cudaError_t fp64_cfl_boundary(const HydroArgs &a, cudaStream_t s);
 cudaError_t fp64_aos_to_soa(const double *aos, double *const q[5], long long n, cudaStream_t s);
 cudaError_t fp64_soa_to_aos(const double *const q[5], double *aos, long long n, cudaStream_t s);
+// opt-in MUSCL-Hancock interior update (FP64) -- hydro_plm.cu; pl: 20 n doubles of scratch
+cudaError_t fp64_plm_interior(const HydroArgs &a, double *pl, cudaStream_t s);
 
 // FP32 hydro path -- hydro_fp32.cu
 cudaError_t fp32_cfl_full(const HydroArgs &a, cudaStream_t s);

@@ -98,6 +98,7 @@ GodunovHLLC3D *solver3d_create_from_deck(const InputDeck *d)   /* hydro_solver_3
     s->lmax = d->grav_lmax;
     s->warm_start = d->warm_start;
     s->sor_depth = d->sor_depth;
+    s->recon = d->recon;
     s->max_steps = d->max_steps;
     s->log_every = d->log_every > 0 ? d->log_every : 10;
     strncpy(s->unet_weights, d->unet_weights, sizeof s->unet_weights - 1);
@@ -130,6 +131,7 @@ static int ensure_device(GodunovHLLC3D *s)
     c.lmax = s->lmax;
     c.warm_start = s->warm_start;
     c.sor_depth = s->sor_depth;
+    c.recon = s->recon;
     if (s->gravity_solver) {
         c.omega = s->gravity_solver->omega;
         c.max_iter = s->gravity_solver->max_iterations;

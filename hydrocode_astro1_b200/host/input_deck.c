@@ -61,7 +61,7 @@ BCType parse_bc_type(const char *str)   /* input_deck.c:45-52 */
     return BC_OUTFLOW;
 }
 
-enum Kind { K_INT, K_DBL, K_BOOL, K_STR, K_PROBLEM, K_BC, K_PRECISION, K_MOMENTS, K_WARM };
+enum Kind { K_INT, K_DBL, K_BOOL, K_STR, K_PROBLEM, K_BC, K_PRECISION, K_MOMENTS, K_WARM, K_RECON };
 
 typedef struct {
     const char *key;
@@ -124,6 +124,7 @@ static const Field FIELDS[] = {
     F("max_steps", K_INT, max_steps), F("log_every", K_INT, log_every),
     F("log_normal_noise", K_DBL, log_noise), F("sor_depth", K_INT, sor_depth),
     F("checkpoint_every", K_INT, checkpoint_every), F("checkpoint_file", K_STR, checkpoint_file),
+    F("reconstruction", K_RECON, recon),
 };
 
 static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
@@ -192,6 +193,7 @@ static void assign(InputDeck *d, const Field *f, const char *v)
         break;
     case K_MOMENTS: *(int *)p = (strcmp(v, "tree") == 0 || strcmp(v, "1") == 0) ? 1 : 0; break;
     case K_WARM: *(int *)p = (strcmp(v, "unet") == 0 || strcmp(v, "1") == 0) ? 1 : 0; break;
+    case K_RECON: *(int *)p = (strcmp(v, "plm") == 0 || strcmp(v, "muscl") == 0 || strcmp(v, "1") == 0) ? 1 : 0; break;
     }
 }
 

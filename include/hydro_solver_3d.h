@@ -89,6 +89,7 @@ typedef struct GodunovHLLC3D {
     char checkpoint_file[256];
     int ck_restored;           /* a binary checkpoint was loaded: its time is ck_t */
     double ck_t;
+    int recon;                 /* 0 piecewise-constant states, 1 MUSCL-Hancock (fp64) */
 } GodunovHLLC3D;
 
 GodunovHLLC3D *solver3d_create(int nx, int ny, int nz,

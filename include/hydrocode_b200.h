@@ -99,6 +99,11 @@ typedef struct hc_config {
     int device;              /* CUDA device ordinal */
     int gravity_only;        /* 1: Poisson solver only (no hydro state); allows
                                 nz == 1, the reference's 2D mode */
+    int recon;               /* interface states: 0 (default) piecewise constant,
+                                the reference's scheme; 1 MUSCL-Hancock
+                                (minmod-limited linear primitives with a half-step
+                                predictor), HC_FP64 only -- no reference
+                                counterpart */
 } hc_config;
 
 typedef struct hc_diag {

@@ -138,6 +138,7 @@ typedef struct {
     int sor_depth;              /* sor_depth: SOR kernels, as hc_config.sor_depth (0 = default) */
     int checkpoint_every;       /* checkpoint_every: binary checkpoint every N steps (0 = off) */
     char checkpoint_file[256];  /* checkpoint_file (default checkpoint.ckpt; the latest one is kept) */
+    int recon;                  /* reconstruction = constant | plm (MUSCL-Hancock, fp64 only) */
 } InputDeck;
 
 InputDeck *input_deck_create(const char *filename);

@@ -604,6 +604,100 @@ static void hydro_bc(hco_grid *g)
     }
 }
 
+/* ---- MUSCL-Hancock face states (no reference counterpart; the reference's
+ * states are piecewise constant, hydro_solver_3d.c:654-724).  Per cell, on
+ * primitives (rho, u, v, w, p):
+ *   slopes  dW_a = minmod(W - W[-e_a], W[+e_a] - W), zero where the cell is
+ *           on the domain boundary along axis a;
+ *   half step (primitive Euler equations, normal velocity un = W.v[a])
+ *           t_a = (un drho + rho du_a,  un du_c for c != a,  un du_a + dp/rho,
+ *                  un dp + gamma p du_a),
+ *           W* = W - h_x t_x - h_y t_y - h_z t_z,  h_a = 0.5 dt / d_a;
+ *   faces   W* + dW_a/2 (the +a face), W* - dW_a/2 (the -a face);
+ *   first order for the cell (W* = W, dW = 0) if W* or any face state has
+ *           rho <= 0 or p <= 0.
+ * The face flux is HLLC on the two face states turned into conserved states.
+ * The CUDA path (hydro_plm.cu) forms the same values in the same order. */
+static inline double minmod(double a, double b)
+{
+    return (a * b <= 0.0) ? 0.0 : (fabs(a) < fabs(b) ? a : b);
+}
+
+static inline void prim_arr(prim_t w, double *o)
+{
+    o[0] = w.d; o[1] = w.v[0]; o[2] = w.v[1]; o[3] = w.v[2]; o[4] = w.p;
+}
+
+static inline cons_t cons_of_arr(const double *o, double gam)
+{
+    prim_t w = { o[0], { o[1], o[2], o[3] }, o[4] };
+    return to_cons(w, gam);
+}
+
+/* pl: 20 arrays of n values -- W* (5), then dW for axes x, y, z (5 each) */
+static void plm_predict(const hco_grid *g, double *pl)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    const size_t n = (size_t)nx * ny * nz;
+    const size_t str[3] = { (size_t)ny * nz, (size_t)nz, 1 };
+    const int nn[3] = { nx, ny, nz };
+    const double gam = g->gamma;
+    const double h[3] = { 0.5 * g->dt / g->dx, 0.5 * g->dt / g->dy, 0.5 * g->dt / g->dz };
+    for (int i = 0; i < nx; i++)
+        for (int j = 0; j < ny; j++)
+            for (int k = 0; k < nz; k++) {
+                const size_t c = at(g, i, j, k);
+                const int idx[3] = { i, j, k };
+                double w[5], dw[3][5], t[3][5], ws[5];
+                prim_arr(to_prim(load(g, c), gam), w);
+                for (int a = 0; a < 3; a++) {
+                    if (idx[a] >= 1 && idx[a] <= nn[a] - 2) {
+                        double wm[5], wp[5];
+                        prim_arr(to_prim(load(g, c - str[a]), gam), wm);
+                        prim_arr(to_prim(load(g, c + str[a]), gam), wp);
+                        for (int v = 0; v < 5; v++) dw[a][v] = minmod(w[v] - wm[v], wp[v] - w[v]);
+                    } else {
+                        for (int v = 0; v < 5; v++) dw[a][v] = 0.0;
+                    }
+                }
+                for (int a = 0; a < 3; a++) {
+                    const double un = w[1 + a];
+                    t[a][0] = un * dw[a][0] + w[0] * dw[a][1 + a];
+                    for (int cc = 0; cc < 3; cc++) t[a][1 + cc] = un * dw[a][1 + cc];
+                    t[a][1 + a] = un * dw[a][1 + a] + dw[a][4] / w[0];
+                    t[a][4] = un * dw[a][4] + gam * w[4] * dw[a][1 + a];
+                }
+                for (int v = 0; v < 5; v++) ws[v] = w[v] - h[0] * t[0][v] - h[1] * t[1][v] - h[2] * t[2][v];
+                int ok = ws[0] > 0.0 && ws[4] > 0.0;
+                for (int a = 0; a < 3; a++) {
+                    ok = ok && (ws[0] + 0.5 * dw[a][0]) > 0.0 && (ws[4] + 0.5 * dw[a][4]) > 0.0;
+                    ok = ok && (ws[0] - 0.5 * dw[a][0]) > 0.0 && (ws[4] - 0.5 * dw[a][4]) > 0.0;
+                }
+                if (!ok) {
+                    for (int v = 0; v < 5; v++) {
+                        ws[v] = w[v];
+                        for (int a = 0; a < 3; a++) dw[a][v] = 0.0;
+                    }
+                }
+                for (int v = 0; v < 5; v++) {
+                    pl[v * n + c] = ws[v];
+                    for (int a = 0; a < 3; a++) pl[(5 + 5 * a + v) * n + c] = dw[a][v];
+                }
+            }
+}
+
+/* flux through the face between cell cl and cl + e_a from the two face states */
+static cons_t plm_flux(const hco_grid *g, const double *pl, size_t cl, size_t cr, int a)
+{
+    const size_t n = (size_t)g->nx * g->ny * g->nz;
+    double L[5], R[5];
+    for (int v = 0; v < 5; v++) {
+        L[v] = pl[v * n + cl] + 0.5 * pl[(5 + 5 * a + v) * n + cl];
+        R[v] = pl[v * n + cr] - 0.5 * pl[(5 + 5 * a + v) * n + cr];
+    }
+    return hllc(cons_of_arr(L, g->gamma), cons_of_arr(R, g->gamma), a, g->gamma);
+}
+
 int hco_step(hco_grid *g)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
@@ -630,6 +724,11 @@ int hco_step(hco_grid *g)
     for (int a = 0; a < 3; a++)
         for (int v = 0; v < 5; v++) F[a][v] = (double *)calloc(n, sizeof(double));
     const size_t str[3] = { (size_t)ny * nz, (size_t)nz, 1 };
+    double *pl = NULL;
+    if (g->recon == 1) {
+        pl = (double *)malloc(20 * n * sizeof(double));
+        plm_predict(g, pl);
+    }
     for (int i = 0; i < nx; i++)
         for (int j = 0; j < ny; j++)
             for (int k = 0; k < nz; k++) {
@@ -637,7 +736,7 @@ int hco_step(hco_grid *g)
                 int lim[3] = { i < nx - 1, j < ny - 1, k < nz - 1 };
                 for (int a = 0; a < 3; a++) {
                     if (!lim[a]) continue;
-                    cons_t f = hllc(load(g, c), load(g, c + str[a]), a, gam);
+                    cons_t f = pl ? plm_flux(g, pl, c, c + str[a], a) : hllc(load(g, c), load(g, c + str[a]), a, gam);
                     F[a][0][c] = f.d; F[a][1][c] = f.m[0]; F[a][2][c] = f.m[1];
                     F[a][3][c] = f.m[2]; F[a][4][c] = f.e;
                 }
@@ -663,6 +762,7 @@ int hco_step(hco_grid *g)
             }
     for (int a = 0; a < 3; a++)
         for (int v = 0; v < 5; v++) free(F[a][v]);
+    free(pl);
 
     /* apply_gravity_source_terms, hydro_solver_3d.c:597-631 (all cells) */
     if (g->gravity) {

@@ -36,6 +36,9 @@ typedef struct hco_grid {
     double dt;
     int last_iter;
     double last_res;
+    int recon;                  /* 0: the reference's piecewise-constant states; 1: MUSCL-Hancock
+                                   (minmod-limited linear primitives, half-step predictor; no
+                                   reference counterpart) */
 } hco_grid;
 
 /* One godunov_step_3d (hydro_solver_3d.c:637-811). Returns SOR status (0 ok,

@@ -41,6 +41,7 @@ class _Grid(C.Structure):
         ("max_iter", C.c_int),
         ("q", _dp * 5), ("phi", _dp), ("gx", _dp), ("gy", _dp), ("gz", _dp),
         ("dt", C.c_double), ("last_iter", C.c_int), ("last_res", C.c_double),
+        ("recon", C.c_int),
     ]
 
 
@@ -80,7 +81,7 @@ class OracleSim:
 
     def __init__(self, nx, ny, nz, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
                  G=0.0, gamma=5.0 / 3.0, cfl=0.4, bc=(2, 2, 2, 2, 2, 2),
-                 omega=1.5, max_iter=10000, tol=1e-6, grav_bc=1, lmax=0):
+                 omega=1.5, max_iter=10000, tol=1e-6, grav_bc=1, lmax=0, recon=0):
         self.lib = oracle_lib()
         self.shape = (nx, ny, nz)
         n = nx * ny * nz
@@ -103,6 +104,7 @@ class OracleSim:
         g.grav_bc = grav_bc
         g.lmax = lmax
         g.omega, g.tol, g.max_iter = omega, tol, max_iter
+        g.recon = recon
         for v in range(5):
             g.q[v] = _ptr(self.q[v])
         g.phi, g.gx, g.gy, g.gz = (_ptr(self.phi), _ptr(self.gx), _ptr(self.gy), _ptr(self.gz))
