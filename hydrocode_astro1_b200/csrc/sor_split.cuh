@@ -96,13 +96,13 @@ __device__ __forceinline__ void pdl_wait_and_release()
 }
 
 template <typename K, typename... Args>
-cudaError_t launch_pdl(K kernel, dim3 grid, dim3 block, cudaStream_t s, Args... args)
+cudaError_t launch_pdl_smem(K kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args)
 {
 #if HC_SOR_PDL
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -111,9 +111,15 @@ cudaError_t launch_pdl(K kernel, dim3 grid, dim3 block, cudaStream_t s, Args... 
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kernel, args...);
 #else
-    kernel<<<grid, block, 0, s>>>(args...);
+    kernel<<<grid, block, smem, s>>>(args...);
     return cudaGetLastError();
 #endif
+}
+
+template <typename K, typename... Args>
+cudaError_t launch_pdl(K kernel, dim3 grid, dim3 block, cudaStream_t s, Args... args)
+{
+    return launch_pdl_smem(kernel, grid, block, 0, s, args...);
 }
 
 // One thread owns the column (j, m) over NI consecutive planes i0..i0+NI-1:

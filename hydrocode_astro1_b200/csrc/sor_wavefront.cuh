@@ -39,15 +39,22 @@ template <> struct SorCoef<double> {
         return old + om * (nw - old);
     }
 };
-// FP32 correction sweep: e_GS = cx (e_x- + e_x+) + cy (..) + cz (..) + delta
+// FP32 correction sweep: e_GS = cx (e_x- + e_x+) + cy (..) + cz (..) + delta.
+// The multiply-adds are written out (fmaf), so every FP32 sweep kernel --
+// scalar, vector, streaming and the two-iteration pass -- rounds each update
+// the same way and they produce the same iterates bit for bit, whatever the
+// compiler would contract in each.
 template <> struct SorCoef<float> {
     float cx, cy, cz, om;
     __device__ __forceinline__ float update(float old, float xm, float xp, float ym, float yp,
                                             float zm, float zp, float src, float &r) const
     {
-        float gs = (xm + xp) * cx + (ym + yp) * cy + (zm + zp) * cz + src;
-        r = fabsf(gs - old);
-        return old + om * (gs - old);
+        const float gs = __fadd_rn(__fmaf_rn(__fadd_rn(zm, zp), cz,
+                                             __fmaf_rn(__fadd_rn(ym, yp), cy, __fmul_rn(__fadd_rn(xm, xp), cx))),
+                                   src);
+        const float d = __fsub_rn(gs, old);
+        r = fabsf(d);
+        return __fmaf_rn(om, d, old);
     }
 };
 

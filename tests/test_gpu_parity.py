@@ -231,12 +231,13 @@ def test_mixed_precision_poisson_converges(depth):
     assert np.abs(phi - o.phi).max() < 2e-4 * np.abs(o.phi).max()
 
 
-@pytest.mark.parametrize("shape", [(40, 37, 72), (130, 20, 32), (24, 60, 40), (70, 70, 64)])
+@pytest.mark.parametrize("shape", [(40, 37, 72), (130, 20, 32), (24, 60, 40), (70, 70, 64), (10, 12, 392)])
 def test_mixed_two_iteration_passes_match_sweeps(shape):
     """The colour-split passes of two iterations each (sor_depth -2: row tiles,
     plane chunks, recomputed halo rows and planes, out of place) give the
-    iterates of the per-colour sweeps: after the same even number of
-    correction iterations the potentials agree to FP32 rounding."""
+    iterates of the per-colour vector sweeps (nz = 392: the longest rows the
+    pass's shared-memory rings hold): after the same even number of correction
+    iterations the potentials are identical."""
     q0, gam = ics.polytrope_n1(shape, R=0.3)
     phis, norms = [], []
     for depth in (0, -2):
@@ -248,9 +249,10 @@ def test_mixed_two_iteration_passes_match_sweeps(shape):
         assert d["last_iterations"] == 30, d
         phis.append(s.phi())
         norms.append(d["last_residual"])
-    diff = np.abs(phis[0] - phis[1]).max()
-    assert diff <= 1e-6 * np.abs(phis[0]).max(), diff
-    assert abs(norms[0] - norms[1]) <= 1e-5 * norms[0], norms
+    # every FP32 sweep kernel forms the update with the same explicit
+    # multiply-adds, so the iterates are the same bits
+    assert np.array_equal(phis[0], phis[1]), np.abs(phis[0] - phis[1]).max()
+    assert norms[0] == norms[1], norms
 
 
 def test_fp32_sod_close_to_fp64():
