@@ -110,6 +110,8 @@ CAPI = {
     "hc_set_unet_record_cycle": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_checkpoint_save": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_longlong]),
     "hc_checkpoint_wait": (C.c_int, [C.c_void_p]),
+    "hc_ic_profile_stars": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_dp), C.POINTER(_dp),
+                                      C.POINTER(_dp), _dp, _dp, _dp]),
     "hc_checkpoint_load": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     "hc_unet_train": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint, C.POINTER(C.c_double)]),
     "hc_unet_loss_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
@@ -360,6 +362,22 @@ class HydroSolver3D:
         the background; the solver may keep stepping.  checkpoint_wait()
         returns when the file is complete."""
         _check(self.L.hc_checkpoint_save(self.h, os.fsencode(path), float(t), int(step)), "hc_checkpoint_save")
+
+    def ic_profile_stars(self, profiles, centres, R_star=None, vel=None):
+        """Initial state built on the device from radial profiles: one star
+        (profiles = [(r, rho, u)], centres = [(x, y, z)]) or two (with R_star
+        and vel per star), as the stellar-profile / binary-star set-ups."""
+        ns = len(profiles)
+        tabs = [tuple(np.ascontiguousarray(a, dtype=np.float64) for a in pr) for pr in profiles]
+        n = (C.c_int * ns)(*[len(t[0]) for t in tabs])
+        rr = (_dp * ns)(*[_p(t[0]) for t in tabs])
+        rh = (_dp * ns)(*[_p(t[1]) for t in tabs])
+        uu = (_dp * ns)(*[_p(t[2]) for t in tabs])
+        cen = np.ascontiguousarray(np.asarray(centres, dtype=np.float64).ravel())
+        Rs = None if R_star is None else np.ascontiguousarray(np.asarray(R_star, dtype=np.float64))
+        vv = None if vel is None else np.ascontiguousarray(np.asarray(vel, dtype=np.float64).ravel())
+        _check(self.L.hc_ic_profile_stars(self.h, ns, n, rr, rh, uu, None if Rs is None else _p(Rs), _p(cen),
+                                          None if vv is None else _p(vv)), "hc_ic_profile_stars")
 
     def checkpoint_wait(self):
         _check(self.L.hc_checkpoint_wait(self.h), "hc_checkpoint_wait")

@@ -1664,3 +1664,32 @@ extern "C" int hc_checkpoint_load(hc_ctx *c, const char *path, double *t, long l
     if (step) *step = h.step;
     return sync_ctx(c);
 }
+
+// ---------------------------------------------------------------- device ICs
+extern "C" int hc_ic_profile_stars(hc_ctx *c, int nstars, const int *n, const double *const *r,
+                                   const double *const *rho, const double *const *u, const double *R_star,
+                                   const double *centre, const double *vel)
+{
+    if (c && c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    if (!c || (nstars != 1 && nstars != 2) || !n || !r || !rho || !u || !centre ||
+        (nstars == 2 && (!R_star || !vel)))
+        return set_err(HC_ERR_ARG, "bad argument (1 or 2 stars; two stars need R_star and vel)");
+    size_t tot = 0;
+    for (int t = 0; t < nstars; t++) {
+        if (n[t] < 2 || !r[t] || !rho[t] || !u[t]) return set_err(HC_ERR_ARG, "a profile needs >= 2 points");
+        for (int q = 0; q + 1 < n[t]; q++)
+            if (!(r[t][q + 1] > r[t][q])) return set_err(HC_ERR_ARG, "profile radii must increase");
+        tot += 3 * (size_t)n[t];
+    }
+    CK(cudaSetDevice(c->dev));
+    double *tmp = nullptr;
+    if (dmalloc((void **)&tmp, tot * sizeof(double))) return set_err(HC_ERR_NOMEM, "profile tables");
+    const bool f64 = c->cfg.precision == HC_FP64;
+    cudaError_t e = ic_profile_stars(c->g, c->cfg.gamma, nstars, n, r, rho, u, R_star, centre, vel,
+                                     f64 ? c->q64[c->cur] : nullptr, f64 ? nullptr : c->q32[c->cur], tmp, c->s);
+    int rc = e == cudaSuccess ? sync_ctx(c) : set_err(HC_ERR_CUDA, cudaGetErrorString(e));
+    cudaFree(tmp);
+    c->cfl_valid = 0;
+    c->launches += 1;
+    return rc;
+}

@@ -102,6 +102,11 @@ cudaError_t fp64_bc(const HydroArgs &a, int axis, cudaStream_t s);
 cudaError_t fp64_cfl_boundary(const HydroArgs &a, cudaStream_t s);
 cudaError_t fp64_aos_to_soa(const double *aos, double *const q[5], long long n, cudaStream_t s);
 cudaError_t fp64_soa_to_aos(const double *const q[5], double *aos, long long n, cudaStream_t s);
+// profile-based initial state on the device -- ics_device.cu
+cudaError_t ic_profile_stars(const Geom &g, double gamma, int nstars, const int *n, const double *const *r,
+                             const double *const *rho, const double *const *u, const double *R_star,
+                             const double *centre, const double *vel, double *const q64[5], float *const q32[5],
+                             double *scratch, cudaStream_t s);
 // opt-in MUSCL-Hancock interior update (FP64) -- hydro_plm.cu; pl: 20 n doubles of scratch
 cudaError_t fp64_plm_interior(const HydroArgs &a, double *pl, cudaStream_t s);
 

@@ -42,6 +42,7 @@ GodunovHLLC3D *solver3d_create(int nx, int ny, int nz, double xmin, double xmax,
     s->enable_gravity = (G > 0.0);
     s->bc_xmin = s->bc_xmax = s->bc_ymin = s->bc_ymax = s->bc_zmin = s->bc_zmax = BC_OUTFLOW;
     s->log_every = 10;
+    s->device_ics = -1;   /* profile set-ups on the device from 256^3 cells on */
     s->gravity_solver = NULL;
     if (s->enable_gravity) {
         s->gravity_solver = gravity_solver_create(nx, ny, nz, xmin, xmax, ymin, ymax, zmin, zmax, G);
@@ -99,6 +100,7 @@ GodunovHLLC3D *solver3d_create_from_deck(const InputDeck *d)   /* hydro_solver_3
     s->warm_start = d->warm_start;
     s->sor_depth = d->sor_depth;
     s->recon = d->recon;
+    s->device_ics = d->device_ics;
     s->max_steps = d->max_steps;
     s->log_every = d->log_every > 0 ? d->log_every : 10;
     strncpy(s->unet_weights, d->unet_weights, sizeof s->unet_weights - 1);
@@ -183,7 +185,9 @@ int solver3d_sync_host(GodunovHLLC3D *s)
         fprintf(stderr, "Error: state download failed: %s\n", hc_last_error());
         return -1;
     }
-    if (s->enable_gravity) {
+    /* g exists once a solve has run (or a checkpoint restored one); before the
+     * first step the host arrays keep their initial zeros */
+    if (s->enable_gravity && s->steps_taken > 0) {
         hc_get_accel(s->dev, s->gx, s->gy, s->gz);
         if (s->gravity_solver) {
             GravitySolver3D *g = s->gravity_solver;
@@ -255,18 +259,47 @@ int solver3d_read_checkpoint(GodunovHLLC3D *s, const char *path, double *t, long
 }
 
 /* ---------------------------------------------------------------- ICs */
+int hc_ic_stars_device(GodunovHLLC3D *s, int nstars, const int *n, const double *const *r,
+                       const double *const *rho, const double *const *u, const double *R_star,
+                       const double *centre, const double *vel)
+{
+    const long long cells = (long long)s->nx * s->ny * s->nz;
+    if (s->device_ics == 0 || (s->device_ics < 0 && cells < (1LL << 24))) return -1;
+    if (ensure_device(s)) return -1;
+    if (hc_ic_profile_stars(s->dev, nstars, n, r, rho, u, R_star, centre, vel) != HC_OK) {
+        fprintf(stderr, "Warning: device initial conditions failed (%s); building them on the host\n",
+                hc_last_error());
+        return -1;
+    }
+    s->ic_on_device = 1;
+    return 0;
+}
+
+/* after a set-up: the host array is newer, unless the state was built on the device */
+static void ic_done(GodunovHLLC3D *s)
+{
+    if (s->ic_on_device) {
+        s->host_dirty = 0;
+        s->device_dirty = 1;
+    } else {
+        s->host_dirty = 1;
+        s->device_dirty = 0;
+    }
+    s->ic_on_device = 0;
+}
+
 void set_initial_conditions_3d(GodunovHLLC3D *s, ProblemType problem)
 {
+    s->ic_on_device = 0;
     hc_ic_problem(s, problem);
-    s->host_dirty = 1;
-    s->device_dirty = 0;
+    ic_done(s);
 }
 
 void set_initial_conditions_3d_from_deck(GodunovHLLC3D *s, const InputDeck *d)
 {
+    s->ic_on_device = 0;
     hc_ic_from_deck(s, d);
-    s->host_dirty = 1;
-    s->device_dirty = 0;
+    ic_done(s);
 }
 
 /* ---------------------------------------------------------------- output */

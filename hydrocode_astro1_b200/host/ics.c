@@ -177,6 +177,14 @@ static void ic_stellar_profile(GodunovHLLC3D *s, const char *fn)   /* :927-1002 
         return;
     }
     double x0 = 0.5 * (s->xmin + s->xmax), y0 = 0.5 * (s->ymin + s->ymax), z0 = 0.5 * (s->zmin + s->zmax);
+    {
+        const double c[3] = { x0, y0, z0 };
+        const double *r = p->r, *rho = p->rho, *u = p->u;
+        if (hc_ic_stars_device(s, 1, &p->n, &r, &rho, &u, NULL, c, NULL) == 0) {
+            profile_free(p);
+            return;
+        }
+    }
     for (int i = 0; i < s->nx; i++)
         for (int j = 0; j < s->ny; j++)
             for (int k = 0; k < s->nz; k++) {
@@ -199,6 +207,14 @@ static void place_two_stars(GodunovHLLC3D *s, const Profile *p1, const Profile *
                             const double v1[3], const double v2[3])
 {
     const double gm1 = s->gamma - 1.0;
+    {
+        const int n[2] = { p1->n, p2->n };
+        const double *r[2] = { p1->r, p2->r }, *rho[2] = { p1->rho, p2->rho }, *u[2] = { p1->u, p2->u };
+        const double R[2] = { p1->R_star, p2->R_star };
+        const double c[6] = { c1[0], c1[1], c1[2], c2[0], c2[1], c2[2] };
+        const double v[6] = { v1[0], v1[1], v1[2], v2[0], v2[1], v2[2] };
+        if (hc_ic_stars_device(s, 2, n, r, rho, u, R, c, v) == 0) return;
+    }
     for (int i = 0; i < s->nx; i++)
         for (int j = 0; j < s->ny; j++)
             for (int k = 0; k < s->nz; k++) {
@@ -639,6 +655,8 @@ void hc_ic_problem(GodunovHLLC3D *s, ProblemType problem)
 /* set_initial_conditions_3d_from_deck, hydro_solver_3d.c:2092-2133 */
 void hc_ic_from_deck(GodunovHLLC3D *s, const InputDeck *d)
 {
+    const int want = s->device_ics;
+    if (d->log_noise > 0.0) s->device_ics = 0;   /* the noise is applied to the host array */
     if (d->problem == STELLAR_OCTANT_EXPLOSION_3D) {
         ic_octant(s, d->stellar_profile, d->explosion_energy, d->explosion_radius, d->explosion_type);
         if (d->enable_perturbations) perturb_octant(s, d);
@@ -649,4 +667,5 @@ void hc_ic_from_deck(GodunovHLLC3D *s, const InputDeck *d)
         hc_ic_problem(s, d->problem);
     }
     if (d->log_noise > 0.0) hc_ic_log_normal(s, d->log_noise, d->perturbation_seed);
+    s->device_ics = want;
 }

@@ -124,7 +124,7 @@ static const Field FIELDS[] = {
     F("max_steps", K_INT, max_steps), F("log_every", K_INT, log_every),
     F("log_normal_noise", K_DBL, log_noise), F("sor_depth", K_INT, sor_depth),
     F("checkpoint_every", K_INT, checkpoint_every), F("checkpoint_file", K_STR, checkpoint_file),
-    F("reconstruction", K_RECON, recon),
+    F("reconstruction", K_RECON, recon), F("device_ics", K_INT, device_ics),
 };
 
 static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
@@ -174,6 +174,7 @@ static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
     d->grav_max_iter = 10000;
     d->log_every = 10;
     strcpy(d->checkpoint_file, "checkpoint.ckpt");
+    d->device_ics = -1;
 }
 
 static int is_true(const char *v) { return strcmp(v, "true") == 0 || strcmp(v, "1") == 0; }

@@ -90,6 +90,9 @@ typedef struct GodunovHLLC3D {
     int ck_restored;           /* a binary checkpoint was loaded: its time is ck_t */
     double ck_t;
     int recon;                 /* 0 piecewise-constant states, 1 MUSCL-Hancock (fp64) */
+    int device_ics;            /* profile-based set-ups built on the device: 1 always, 0 never,
+                                  -1 (default) from 256^3 cells on */
+    int ic_on_device;          /* the last set-up left the state on the device only */
 } GodunovHLLC3D;
 
 GodunovHLLC3D *solver3d_create(int nx, int ny, int nz,

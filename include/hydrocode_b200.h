@@ -253,6 +253,19 @@ int hc_checkpoint_save(hc_ctx *ctx, const char *path, double t, long long step);
 int hc_checkpoint_wait(hc_ctx *ctx);
 int hc_checkpoint_load(hc_ctx *ctx, const char *path, double *t, long long *step);
 
+/* Initial state of the stellar-profile (nstars = 1: every cell from the
+ * profile at its distance to centre[0..2], at rest) or binary-star (nstars =
+ * 2: inside one star -- r < R_star[s] -- its profile and velocity vel[3s..];
+ * inside both the density-weighted mix; outside both the floors) set-ups,
+ * built on the device from radial profile tables (r strictly increasing,
+ * n[s] points, rho and specific internal energy u), as
+ * hydro_solver_3d.c:927-1002 and :1133-1205 define them.  No reference
+ * counterpart as an entry point: the reference loops over the cells on the
+ * host.  The state equals what hc_set_state would set from the host-built
+ * array, bit for bit, without that array or its upload. */
+int hc_ic_profile_stars(hc_ctx *ctx, int nstars, const int *n, const double *const *r, const double *const *rho,
+                        const double *const *u, const double *R_star, const double *centre, const double *vel);
+
 /* Diagnostics of the tensor-core convolution kernels (no reference
  * counterpart), on host buffers.  Volumes are nx*ny*nz voxels of 16 BF16
  * channels (channels last), weights w[co][tap][ci] (16*27*16 BF16, tap =

@@ -139,6 +139,7 @@ typedef struct {
     int checkpoint_every;       /* checkpoint_every: binary checkpoint every N steps (0 = off) */
     char checkpoint_file[256];  /* checkpoint_file (default checkpoint.ckpt; the latest one is kept) */
     int recon;                  /* reconstruction = constant | plm (MUSCL-Hancock, fp64 only) */
+    int device_ics;             /* device_ics: profile set-ups on the device (1), host (0), auto (-1, default) */
 } InputDeck;
 
 InputDeck *input_deck_create(const char *filename);
