@@ -266,8 +266,11 @@ __device__ __forceinline__ void lin_coarse(int i, int n0, int &a, int &b, float 
 // e (colour-split FP32, whole grid) = trilinear upsample of the network output
 // times rms * kscale; zero on boundary cells.  A CTA takes OUT_UP_ROWS
 // consecutive (i, j) rows; per row the coarse rows and weights in i and j are
-// fixed, and thread m writes the cells k = 2m and 2m+1 (one of each colour;
-// consecutive m are consecutive in each colour array).
+// fixed, and thread m writes the cells k = 2m (colour (i+j)&1) and k = 2m+1
+// (the other colour), both at index m of their colour array.  Their k
+// neighbours in the coarse rows are columns m-1, m (k = 2m, weight 0.75 on m)
+// and m, m+1 (k = 2m+1, weight 0.25 on m+1), clamped at the ends: twelve
+// loads serve both cells, each formed in the order k, then j, then i.
 constexpr int OUT_UP_ROWS = 16;
 __global__ void out_up_kernel(const float *__restrict__ out0, Dims d0, const double *__restrict__ sumsq, float kscale,
                               Split sp, float *__restrict__ e)
@@ -275,6 +278,7 @@ __global__ void out_up_kernel(const float *__restrict__ out0, Dims d0, const dou
     const double ms = *sumsq / (double)d0.n;
     const float sc = (float)sqrt(ms) * kscale;
     const long long rows = (long long)sp.nx * sp.ny;
+    const int n0 = d0.nz;
     for (int q = 0; q < OUT_UP_ROWS; q++) {
         const long long row = (long long)blockIdx.x * OUT_UP_ROWS + q;   // i * ny + j
         if (row >= rows) break;
@@ -286,25 +290,35 @@ __global__ void out_up_kernel(const float *__restrict__ out0, Dims d0, const dou
         lin_coarse(j, d0.ny, ja, jb, wj);
         const float *p00 = out0 + vidx(d0, ia, ja, 0), *p01 = out0 + vidx(d0, ia, jb, 0);
         const float *p10 = out0 + vidx(d0, ib, ja, 0), *p11 = out0 + vidx(d0, ib, jb, 0);
+        const int cc = (i + j) & 1;   // colour of k = 2m
+        float *e0 = e + cc * sp.cs + row * sp.H, *e1 = e + (cc ^ 1) * sp.cs + row * sp.H;
         for (int m = threadIdx.x; m < sp.H; m += blockDim.x) {
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int k = 2 * m + h;
-                if (k >= sp.nz) break;
-                float val = 0.f;
-                if (rin && k >= 1 && k <= sp.nz - 2) {
-                    int ka, kb;
-                    float wk;
-                    lin_coarse(k, d0.nz, ka, kb, wk);
-                    const float c00 = p00[ka] * (1.f - wk) + p00[kb] * wk;
-                    const float c01 = p01[ka] * (1.f - wk) + p01[kb] * wk;
-                    const float c10 = p10[ka] * (1.f - wk) + p10[kb] * wk;
-                    const float c11 = p11[ka] * (1.f - wk) + p11[kb] * wk;
-                    const float c0 = c00 * (1.f - wj) + c01 * wj, c1 = c10 * (1.f - wj) + c11 * wj;
-                    val = (c0 * (1.f - wi) + c1 * wi) * sc;
+            const int k0 = 2 * m, k1 = 2 * m + 1;
+            const bool in0 = rin && k0 >= 1 && k0 <= sp.nz - 2, in1 = rin && k1 >= 1 && k1 <= sp.nz - 2;
+            float v0 = 0.f, v1 = 0.f;
+            if (in0 || in1) {
+                const int km = max(m - 1, 0), kp = min(m + 1, n0 - 1);
+                const float a00 = p00[km], b00 = p00[m], c00 = p00[kp];
+                const float a01 = p01[km], b01 = p01[m], c01 = p01[kp];
+                const float a10 = p10[km], b10 = p10[m], c10 = p10[kp];
+                const float a11 = p11[km], b11 = p11[m], c11 = p11[kp];
+                if (in0) {   // lin_coarse(2m): (m-1, m), weight 0.75 on m
+                    const float wk = 0.75f;
+                    const float s00 = a00 * (1.f - wk) + b00 * wk, s01 = a01 * (1.f - wk) + b01 * wk;
+                    const float s10 = a10 * (1.f - wk) + b10 * wk, s11 = a11 * (1.f - wk) + b11 * wk;
+                    const float t0 = s00 * (1.f - wj) + s01 * wj, t1 = s10 * (1.f - wj) + s11 * wj;
+                    v0 = (t0 * (1.f - wi) + t1 * wi) * sc;
                 }
-                e[sp.at(i, j, k)] = val;
+                if (in1) {   // lin_coarse(2m+1): (m, m+1), weight 0.25 on m+1
+                    const float wk = 0.25f;
+                    const float s00 = b00 * (1.f - wk) + c00 * wk, s01 = b01 * (1.f - wk) + c01 * wk;
+                    const float s10 = b10 * (1.f - wk) + c10 * wk, s11 = b11 * (1.f - wk) + c11 * wk;
+                    const float t0 = s00 * (1.f - wj) + s01 * wj, t1 = s10 * (1.f - wj) + s11 * wj;
+                    v1 = (t0 * (1.f - wi) + t1 * wi) * sc;
+                }
             }
+            e0[m] = v0;
+            if (k1 < sp.nz) e1[m] = v1;
         }
     }
 }
