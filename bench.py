@@ -357,6 +357,8 @@ def main_ours(args):
     UNET_PASSES = args.unet_passes
     if args.unet_weights:
         UNET_WEIGHTS = os.path.abspath(args.unet_weights)
+        if not os.path.exists(UNET_WEIGHTS):
+            raise SystemExit("bench.py: no weight file %s" % UNET_WEIGHTS)
 
     import hydrocode_astro1_b200 as hc
     world, rank, local, dist = dist_setup(args)

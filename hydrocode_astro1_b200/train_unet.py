@@ -1,7 +1,7 @@
 """Train the warm-start U-Net on the GPU from solves of the plain solver.
 
     python -m hydrocode_astro1_b200.train_unet --problem stellar_explosion --n 256 --seed 7 \\
-        --solves 25 --train-steps 2000 --out hydrocode_astro1_b200/data/unet_stellar_explosion_256.bin
+        --solves 60 --train-steps 9000 --out hydrocode_astro1_b200/data/unet_stellar_explosion_256.bin
 
 Runs `solves` steps of the problem in FP32 + mixed precision with the
 previous-potential warm start (the plain method) for each recorded cycle,
