@@ -495,8 +495,7 @@ def main_ours(args):
 
     # end to end through the C ABI with host buffers (AoS State3D, pinned)
     if not args.no_e2e:
-        from oracle.oracle import soa_to_aos  # layout helper only
-        U = hc.pin(soa_to_aos(s.state() if not fp64 else s.state()))
+        U = hc.pin(s.state_aos())
         ne = min(args.steps, 3)
         barrier(dist)
         t = time.perf_counter()
