@@ -108,6 +108,7 @@ CAPI = {
     "hc_set_unet_passes": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_cycles": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_record_cycle": (C.c_int, [C.c_void_p, C.c_int]),
+    "hc_set_correction_omega": (C.c_int, [C.c_void_p, C.c_double]),
     "hc_checkpoint_save": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_longlong]),
     "hc_checkpoint_wait": (C.c_int, [C.c_void_p]),
     "hc_ic_profile_stars": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(_dp), C.POINTER(_dp),
@@ -392,6 +393,11 @@ class HydroSolver3D:
     def unet_record_cycle(self, c):
         """With collection on: the correction cycle whose residual is recorded."""
         _check(self.L.hc_set_unet_record_cycle(self.h, int(c)), "hc_set_unet_record_cycle")
+
+    def correction_omega(self, omega):
+        """Relaxation factor of the FP32 correction sweeps of the mixed solve
+        (0 < omega < 2; 0: the solve's own omega, the default)."""
+        _check(self.L.hc_set_correction_omega(self.h, float(omega)), "hc_set_correction_omega")
 
     def unet_train(self, steps, lr=1e-3, seed=0):
         loss = C.c_double(0.0)

@@ -109,6 +109,7 @@ struct hc_ctx {
     int unet_passes;             // learned-start predictions per solve (>= 1)
     int unet_cycles;             // correction cycles that start from a prediction (0: 2)
     int unet_record_cycle;       // the cycle whose residual is recorded for training (0: 1)
+    double corr_omega;           // relaxation of the FP32 correction sweeps (0: the solve's omega)
     // checkpoints: device packing buffer, copy stream, writer thread
     unsigned char *ck_dev;
     size_t ck_dev_bytes;
@@ -687,6 +688,10 @@ static int sor_fp64(hc_ctx *c, const double *rho)
 int hc_sor_mixed(hc_ctx *c, const float *rho32)
 {
     GravArgs a = grav_args(c, nullptr, rho32);
+    // only the correction sweeps relax (the FP64 residual and update do not),
+    // so a.omega here is theirs; the stopping test max|phi_GS - phi_old| < tol
+    // does not depend on it
+    if (c->corr_omega > 0.0) a.omega = c->corr_omega;
     // sor_depth 0 (default): colour-split sweeps on e and r; -2: colour-split,
     // two iterations per HBM pass (temporal blocking, out of place between
     // e32 and e32b; colour-split sweeps where the tiling does not fit); -1:
@@ -1426,6 +1431,14 @@ extern "C" int hc_set_unet_record_cycle(hc_ctx *c, int cycle)
 {
     if (!c || cycle < 1 || cycle > 8) return set_err(HC_ERR_ARG, "cycle must be 1..8");
     c->unet_record_cycle = cycle;
+    return HC_OK;
+}
+
+extern "C" int hc_set_correction_omega(hc_ctx *c, double omega)
+{
+    if (!c || !(omega == 0.0 || (omega > 0.0 && omega < 2.0)))
+        return set_err(HC_ERR_ARG, "correction omega must be 0 (the solve's omega) or in (0, 2)");
+    c->corr_omega = omega;
     return HC_OK;
 }
 

@@ -229,6 +229,13 @@ int hc_set_unet_cycles(hc_ctx *ctx, int cycles);
 /* With collection on (hc_unet_collect): the correction cycle whose starting
  * residual is recorded as a training sample (1..8, default 1). */
 int hc_set_unet_record_cycle(hc_ctx *ctx, int cycle);
+/* Relaxation factor of the FP32 correction sweeps of a mixed-precision solve
+ * (0 < omega < 2; 0 restores the default, the solve's own omega).  No
+ * reference counterpart: the reference relaxes every sweep with the one omega
+ * of gravity_set_solver_params (gravity_solver_3d.c:78, :137-144).  The
+ * FP64 path ignores it, and the solve still stops on the reference's test
+ * max|phi_GS - phi_old| < tol, which does not depend on omega. */
+int hc_set_correction_omega(hc_ctx *ctx, double omega);
 
 /* Binary checkpoint and restart.  No counterpart in the reference, whose
  * restart reads its own CSV output (hydro_solver_3d.c:2142-2351): 6 decimal
