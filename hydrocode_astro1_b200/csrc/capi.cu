@@ -30,6 +30,7 @@ using namespace hc;
 // ---------------------------------------------------------------- errors
 static thread_local char g_err[512] = "";
 
+static int set_err(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
 static int set_err(int code, const char *fmt, ...)
 {
     va_list ap;
@@ -1572,7 +1573,7 @@ extern "C" int hc_checkpoint_wait(hc_ctx *c)
     }
     const int st = c->ck_status;
     c->ck_status = HC_OK;
-    if (st) return set_err(st, c->ck_err);
+    if (st) return set_err(st, "%s", c->ck_err);
     return HC_OK;
 }
 
@@ -1624,7 +1625,7 @@ extern "C" int hc_checkpoint_load(hc_ctx *c, const char *path, double *t, long l
     ck_fill_header(c, want);
     auto bad = [&](const char *what) {
         fclose(f);
-        return set_err(HC_ERR_ARG, what);
+        return set_err(HC_ERR_ARG, "%s", what);
     };
     if (fread(&h, sizeof h, 1, f) != 1 || memcmp(h.magic, "HCCKPT01", 8) != 0 || h.version != 1 ||
         h.header_bytes != (int32_t)sizeof(CkptHeader))
@@ -1648,14 +1649,23 @@ extern "C" int hc_checkpoint_load(hc_ctx *c, const char *path, double *t, long l
     for (size_t k = 0; k < nch; k++) {
         const size_t off = k * CK_CHUNK, len = std::min(CK_CHUNK, bytes - off);
         unsigned char *buf = c->ck_host[k & 1];
-        if (k >= 2) CK(cudaEventSynchronize(c->ck_ev[k & 1]));   // the copy out of this buffer is done
+        // the copy out of this buffer (chunk k - 2) is done
+        cudaError_t e = k >= 2 ? cudaEventSynchronize(c->ck_ev[k & 1]) : cudaSuccess;
+        if (e != cudaSuccess) {
+            fclose(f);
+            return set_err(HC_ERR_CUDA, "checkpoint load: %s", cudaGetErrorString(e));
+        }
         if (fread(buf, 1, len, f) != len) {
             cudaStreamSynchronize(c->ck_stream);
             return bad("checkpoint: file is shorter than its header says");
         }
         hash = fnv1a(hash, buf, len);
-        CK(cudaMemcpyAsync(c->ck_dev + off, buf, len, cudaMemcpyHostToDevice, c->ck_stream));
-        CK(cudaEventRecord(c->ck_ev[k & 1], c->ck_stream));
+        e = cudaMemcpyAsync(c->ck_dev + off, buf, len, cudaMemcpyHostToDevice, c->ck_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ck_ev[k & 1], c->ck_stream);
+        if (e != cudaSuccess) {
+            fclose(f);
+            return set_err(HC_ERR_CUDA, "checkpoint load: %s", cudaGetErrorString(e));
+        }
     }
     fclose(f);
     CK(cudaStreamSynchronize(c->ck_stream));
@@ -1700,7 +1710,7 @@ extern "C" int hc_ic_profile_stars(hc_ctx *c, int nstars, const int *n, const do
     const bool f64 = c->cfg.precision == HC_FP64;
     cudaError_t e = ic_profile_stars(c->g, c->cfg.gamma, nstars, n, r, rho, u, R_star, centre, vel,
                                      f64 ? c->q64[c->cur] : nullptr, f64 ? nullptr : c->q32[c->cur], tmp, c->s);
-    int rc = e == cudaSuccess ? sync_ctx(c) : set_err(HC_ERR_CUDA, cudaGetErrorString(e));
+    int rc = e == cudaSuccess ? sync_ctx(c) : set_err(HC_ERR_CUDA, "%s", cudaGetErrorString(e));
     cudaFree(tmp);
     c->cfl_valid = 0;
     c->launches += 1;
