@@ -17,6 +17,7 @@ shock breakout, 2000 steps -- are not repeated here).
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import sys
@@ -88,6 +89,10 @@ def main():
             rec[arm] = dict(r32, density_l1=float(np.abs(q32[0] - q64[0]).mean() / np.abs(q64[0]).mean()),
                             mass_drift=float(q32[0].sum() * dV / m0 - 1),
                             energy_drift=float(q32[4].sum() * dV / e0 - 1))
+            if warm == hc.HC_WARM_UNET:   # which network the learned-start figures belong to
+                with open(WEIGHTS, "rb") as f:
+                    rec[arm]["weights"] = dict(file=os.path.basename(WEIGHTS),
+                                               sha256=hashlib.sha256(f.read()).hexdigest()[:16])
             if c == 1:   # hydrostatic n=1 polytrope: central density and spurious velocities
                 ic = tuple(n // 2 for n in p["shape"])
                 for tag, q in (("fp64", q64), (arm, q32)):
