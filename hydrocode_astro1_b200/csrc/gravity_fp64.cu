@@ -431,13 +431,9 @@ inline int grid_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 cudaError_t grav_moments_sequential(const GravArgs &a, cudaStream_t s)
 {
     const size_t sm = 9 * SEQ_CH * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(moments_seq_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = set_smem_once(attr_set, (const void *)moments_seq_kernel, (int)sm);
+    if (e != cudaSuccess) return e;
     moments_seq_kernel<<<1, SEQ_NT, sm, s>>>(a);
     return cudaGetLastError();
 }
@@ -537,14 +533,9 @@ cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, in
 {
     constexpr size_t sm = sor_wavefront_smem<double, WF64_T, WF64_TJ, WF64_TK>();
     auto kern = sor_wavefront_kernel<double, double, WF64_T, WF64_TJ, WF64_TK, WF64_NT>;
-    static int attr_dev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (attr_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        attr_dev = dev;
-    }
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = set_smem_once(attr_set, (const void *)kern, (int)sm);
+    if (e != cudaSuccess) return e;
     SorCoef<double> cf;
     cf.ix2 = 1.0 / (a.g.dx * a.g.dx);
     cf.iy2 = 1.0 / (a.g.dy * a.g.dy);
@@ -567,12 +558,9 @@ cudaError_t grav_sor_pass64(const GravArgs &a, const double *in, double *out, in
     if (wf_tma_enabled() && tmap3(in, 8, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tin) &&
         tmap3(a.rho, 8, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tsrc)) {
         auto kt = wtma::sor_wavefront_tma_kernel<double, double, WF64_T, WF64_TJ, WF64_TK, WF64_NT>;
-        static int attr_t = -1;
-        if (attr_t != dev) {
-            cudaError_t e = cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM);
-            if (e != cudaSuccess) return e;
-            attr_t = dev;
-        }
+        static std::atomic<unsigned long long> attr_t{0};
+        e = set_smem_once(attr_t, (const void *)kt, (int)SH::SMEM);
+        if (e != cudaSuccess) return e;
         kt<<<grid, WF64_NT, SH::SMEM, s>>>(tin, tsrc, out, a.g, cf, a.res, iter0, a.tol, a.sc, chunk);
         return cudaGetLastError();
     }

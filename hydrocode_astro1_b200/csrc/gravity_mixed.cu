@@ -812,14 +812,9 @@ cudaError_t pass32(const GravArgs &a, const float *in, float *out, const float *
 {
     constexpr size_t sm = sor_wavefront_smem<float, TT, WF32_TJ, WF32_TK>();
     auto kern = sor_wavefront_kernel<float, float, TT, WF32_TJ, WF32_TK, WF32_NT>;
-    static int attr_dev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (attr_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        attr_dev = dev;
-    }
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = set_smem_once(attr_set, (const void *)kern, (int)sm);
+    if (e != cudaSuccess) return e;
     SorCoef<float> cf;
     double ix2 = 1.0 / (a.g.dx * a.g.dx), iy2 = 1.0 / (a.g.dy * a.g.dy), iz2 = 1.0 / (a.g.dz * a.g.dz);
     double fac = 2.0 * (ix2 + iy2 + iz2);
@@ -841,12 +836,9 @@ cudaError_t pass32(const GravArgs &a, const float *in, float *out, const float *
     if (TT >= 2 && wf_tma_enabled() && tmap3(in, 4, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tin) &&
         tmap3(r32, 4, a.g.nx, a.g.ny, a.g.nz, SH::SK, SH::SJ, &tsrc)) {
         auto kt = wtma::sor_wavefront_tma_kernel<float, float, TT, WF32_TJ, WF32_TK, WF32_NT>;
-        static int attr_t = -1;
-        if (attr_t != dev) {
-            cudaError_t e = cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SH::SMEM);
-            if (e != cudaSuccess) return e;
-            attr_t = dev;
-        }
+        static std::atomic<unsigned long long> attr_t{0};
+        e = set_smem_once(attr_t, (const void *)kt, (int)SH::SMEM);
+        if (e != cudaSuccess) return e;
         kt<<<grid, WF32_NT, SH::SMEM, s>>>(tin, tsrc, out, a.g, cf, a.res, iter0, thresh, a.sc, chunk);
         return cudaGetLastError();
     }

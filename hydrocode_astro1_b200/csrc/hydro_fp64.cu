@@ -48,13 +48,9 @@ cudaError_t fp64_dt(const HydroArgs &a, cudaStream_t s)
 cudaError_t fp64_interior(const HydroArgs &a, int chunks, cudaStream_t s)
 {
     constexpr size_t sm = interior_smem<double, TK, TJ>();
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(interior_kernel<double, TK, TJ>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = set_smem_once(attr_set, (const void *)interior_kernel<double, TK, TJ>, (int)sm);
+    if (e != cudaSuccess) return e;
     int nint = a.g.nx - 2;
     int ilen = (nint + chunks - 1) / chunks;
     chunks = (nint + ilen - 1) / ilen;

@@ -4,6 +4,8 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
@@ -82,15 +84,9 @@ cudaError_t conv3(const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *b
 {
     CUtensorMap tm;
     if (halo_enabled() && halo_map(x, d, &tm)) {
-        static int attr_dev = -1;
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (attr_dev != dev) {
-            cudaError_t e = cudaFuncSetAttribute(conv3_halo_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)sizeof(HaloSmem));
-            if (e != cudaSuccess) return e;
-            attr_dev = dev;
-        }
+        static std::atomic<unsigned long long> attr_set{0};
+        cudaError_t e = hc::set_smem_once(attr_set, (const void *)conv3_halo_kernel, (int)sizeof(HaloSmem));
+        if (e != cudaSuccess) return e;
         const int tk = (d.nz + HT_K - 1) / HT_K, tj = (d.ny + HT_J - 1) / HT_J;
         // 6 CTAs per SM (shared-memory limit): as many plane chunks as fit one
         // wave (rounding up would leave a second, nearly empty wave); at least
@@ -113,15 +109,9 @@ cudaError_t conv3(const __nv_bfloat16 *x, const __nv_bfloat16 *w, const float *b
 cudaError_t wgrad(const __nv_bfloat16 *x, const __nv_bfloat16 *dy, float *dw, float *partial, int max_parts,
                   const Dims &d, int *err, cudaStream_t s)
 {
-    static int attr_dev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (attr_dev != dev) {
-        cudaError_t e = cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sizeof(WgradSmem));
-        if (e != cudaSuccess) return e;
-        attr_dev = dev;
-    }
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = hc::set_smem_once(attr_set, (const void *)wgrad_kernel, (int)sizeof(WgradSmem));
+    if (e != cudaSuccess) return e;
     const long long nchunk = (d.n + KC - 1) / KC;
     int parts = (int)std::min<long long>(max_parts, nchunk);
     const int per = (int)((nchunk + parts - 1) / parts);
