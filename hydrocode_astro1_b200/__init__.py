@@ -56,6 +56,9 @@ class Diag(C.Structure):
         ("outer_cycles", C.c_int), ("dt", C.c_double), ("steps", C.c_longlong),
         ("total_iterations", C.c_longlong), ("overshoot", C.c_int),
         ("unet_accepted", C.c_longlong), ("unet_fallbacks", C.c_longlong),
+        ("cons", C.c_double * 5),
+        ("unet_probes", C.c_longlong), ("unet_wins", C.c_longlong), ("unet_losses", C.c_longlong),
+        ("unet_switch_offs", C.c_longlong), ("unet_off", C.c_int),
     ]
 
 
@@ -92,6 +95,8 @@ CAPI = {
     "hc_get_accel": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
     "hc_get_moments": (C.c_int, [C.c_void_p, _dp, C.c_int]),
     "hc_residual_norm": (C.c_int, [C.c_void_p, _dp]),
+    "hc_conservation_sums": (C.c_int, [C.c_void_p, _dp]),
+    "hc_set_conservation_record": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_get_diag": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
     "hc_get_timing": (C.c_int, [C.c_void_p, C.POINTER(Timing), C.c_int]),
     "hc_sync": (C.c_int, [C.c_void_p]),
@@ -107,6 +112,7 @@ CAPI = {
     "hc_unet_samples": (C.c_int, [C.c_void_p]),
     "hc_set_unet_passes": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_cycles": (C.c_int, [C.c_void_p, C.c_int]),
+    "hc_set_unet_guard": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_unet_record_cycle": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_set_correction_omega": (C.c_int, [C.c_void_p, C.c_double]),
     "hc_checkpoint_save": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_longlong]),
@@ -302,10 +308,23 @@ class HydroSolver3D:
         _check(self.L.hc_residual_norm(self.h, C.byref(v)), "hc_residual_norm")
         return v.value
 
+    def conservation(self):
+        """FP64 sums over all cells of (rho, rho u, rho v, rho w, E), formed on
+        the device in a fixed order; times the cell volume they are totals."""
+        out = np.zeros(5)
+        _check(self.L.hc_conservation_sums(self.h, _p(out)), "hc_conservation_sums")
+        return out
+
+    def set_conservation_record(self, on=True):
+        """Form the sums after every hc_step call (hc_diag 'cons')."""
+        _check(self.L.hc_set_conservation_record(self.h, int(bool(on))), "hc_set_conservation_record")
+
     def diagnostics(self):
         d = Diag()
         _check(self.L.hc_get_diag(self.h, C.byref(d)), "hc_get_diag")
-        return {f: getattr(d, f) for f, _ in Diag._fields_}
+        out = {f: getattr(d, f) for f, _ in Diag._fields_}
+        out["cons"] = list(d.cons)
+        return out
 
     def timing(self, reset=False):
         t = Timing()
@@ -353,6 +372,11 @@ class HydroSolver3D:
 
     def unet_passes(self, n):
         _check(self.L.hc_set_unet_passes(self.h, int(n)), "hc_set_unet_passes")
+
+    def unet_guard(self, consecutive_losses=3):
+        """Outcome monitor of the learned start: switch the network off after
+        this many consecutive solves where it saved no iterations (0: off)."""
+        _check(self.L.hc_set_unet_guard(self.h, int(consecutive_losses)), "hc_set_unet_guard")
 
     def unet_cycles(self, n):
         """Correction cycles that start from the network's prediction (default 2)."""

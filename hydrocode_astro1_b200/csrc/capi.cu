@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "hc_internal.cuh"
+#include "unet_guard.h"
 
 #ifndef HC_CYCLE_REDUCTION
 #define HC_CYCLE_REDUCTION 1.0e-4   // residual reduction a correction cycle's sweeps aim for
@@ -111,6 +112,9 @@ struct hc_ctx {
     int unet_cycles;             // correction cycles that start from a prediction (0: 2)
     int unet_record_cycle;       // the cycle whose residual is recorded for training (0: 1)
     double corr_omega;           // relaxation of the FP32 correction sweeps (0: the solve's omega)
+    UnetGuard guard;             // learned-start outcome monitor (hc_set_unet_guard)
+    double *cons_part;           // conservation sums: 5 * CONS_BLOCKS block partials
+    int cons_record;             // 1: sums after every step, reported in hc_diag.cons
     // checkpoints: device packing buffer, copy stream, writer thread
     unsigned char *ck_dev;
     size_t ck_dev_bytes;
@@ -213,7 +217,7 @@ static void free_ctx(hc_ctx *c)
     cudaFree(c->phs); cudaFree(c->rhs); cudaFree(c->plm);
     cudaFree(c->e32); cudaFree(c->r32); cudaFree(c->e32b);
     cudaFree(c->gx); cudaFree(c->gy); cudaFree(c->gz);
-    cudaFree(c->res); cudaFree(c->scratch); cudaFree(c->mom);
+    cudaFree(c->res); cudaFree(c->scratch); cudaFree(c->mom); cudaFree(c->cons_part);
     cudaFree(c->sc); cudaFree(c->stage);
     if (c->hsc) cudaFreeHost(c->hsc);
     if (c->hdt) cudaFreeHost(c->hdt);
@@ -682,6 +686,9 @@ static int sor_fp64(hc_ctx *c, const double *rho)
     return done ? 0 : -1;
 }
 
+static bool guard_allows_prediction(hc_ctx *c) { return unet_guard_allows(c->guard); }
+static void guard_record(hc_ctx *c, bool predicted, int iters) { unet_guard_record(c->guard, predicted, iters); }
+
 // Mixed-precision Poisson solve: FP64 residual of the full potential, FP32
 // red-black SOR on the correction, FP64 update; repeated until the FP64
 // update norm max|delta| is below tol.  Iteration budget: max_iter inner
@@ -726,6 +733,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
     };
     c->diag.warm_start_used = 0;
     bool recorded = false;
+    const bool guard_ok = c->cfg.warm_start == HC_WARM_UNET ? guard_allows_prediction(c) : true;
     while (true) {
         const double prev_dmax = cycles ? dmax : 1e300;
         rc = residual(&dmax);
@@ -743,7 +751,8 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         const int ucycles = c->unet_cycles > 0 ? c->unet_cycles : 2;
         const int rcycle = c->unet_record_cycle > 0 ? c->unet_record_cycle : 1;
         if ((cycles <= ucycles || cycles == rcycle) && split && c->unet && std::isfinite(dmax)) {
-            const bool predict = cycles <= ucycles && c->cfg.warm_start == HC_WARM_UNET && unet_has_weights(c->unet);
+            const bool predict = cycles <= ucycles && c->cfg.warm_start == HC_WARM_UNET && guard_ok &&
+                                 unet_has_weights(c->unet);
             const bool rec = cycles == rcycle && unet_collecting(c->unet);
             if (predict || rec) {
                 {
@@ -911,6 +920,15 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
     c->diag.last_residual = dmax;
     c->diag.outer_cycles = cycles;
     c->diag.total_iterations += total;
+    if (c->cfg.warm_start == HC_WARM_UNET && unet_has_weights(c->unet)) {
+        guard_record(c, c->diag.warm_start_used != 0, total);
+        const UnetGuard &g = c->guard;
+        c->diag.unet_probes = g.probes;
+        c->diag.unet_wins = g.wins;
+        c->diag.unet_losses = g.loss_total;
+        c->diag.unet_switch_offs = g.switch_offs;
+        c->diag.unet_off = g.off;
+    }
     if (recorded) {
         rc = unet_end_solve(c->unet, a, status == 0, c->s);
         if (rc) return set_err(rc, "learned warm start: recording a training sample failed");
@@ -1170,6 +1188,8 @@ static int step_once(hc_ctx *c, int *grav_status)
     return HC_OK;
 }
 
+static int launch_cons_sums(hc_ctx *c);
+
 static int ensure_hdt(hc_ctx *c, int n)
 {
     if (c->hdt && c->hdt_cap >= n) return HC_OK;
@@ -1196,9 +1216,16 @@ extern "C" int hc_step(hc_ctx *c, int nsteps, double *dt_out)
         if (gs == -1) worst = -1;
         CK(cudaMemcpyAsync(c->hdt + q, &c->sc->dt, sizeof(double), cudaMemcpyDeviceToHost, c->s));
     }
+    if (c->cons_record && nsteps > 0) {
+        rc = launch_cons_sums(c);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(c->hsc->cons, c->sc->cons, sizeof c->hsc->cons, cudaMemcpyDeviceToHost, c->s));
+    }
     rc = sync_ctx(c);
     if (rc) return rc;
     if (nsteps > 0) c->diag.dt = c->hdt[nsteps - 1];
+    if (c->cons_record && nsteps > 0)
+        for (int v = 0; v < 5; v++) c->diag.cons[v] = c->hsc->cons[v];
     if (dt_out)
         for (int q = 0; q < nsteps; q++) dt_out[q] = c->hdt[q];
     return worst ? HC_NOT_CONVERGED : HC_OK;
@@ -1230,6 +1257,46 @@ extern "C" int hc_step_host(hc_ctx *c, double *U, double *dt_out)
     c->diag.dt = c->hdt[0];
     if (dt_out) *dt_out = c->hdt[0];
     return gs == -1 ? HC_NOT_CONVERGED : HC_OK;
+}
+
+// FP64 sums of the current state's 5 conserved fields into sc->cons (no sync).
+static int launch_cons_sums(hc_ctx *c)
+{
+    if (!c->cons_part && dmalloc((void **)&c->cons_part, 5 * (size_t)CONS_BLOCKS * sizeof(double)))
+        return set_err(HC_ERR_NOMEM, "conservation-sum partials");
+    if (c->cfg.precision == HC_FP64) {
+        ConsFields<double> q;
+        for (int v = 0; v < 5; v++) q.f[v] = c->q64[c->cur][v];
+        CK(cons_sums(q, c->g.n, c->cons_part, c->sc->cons, c->s));
+    } else {
+        ConsFields<float> q;
+        for (int v = 0; v < 5; v++) q.f[v] = c->q32[c->cur][v];
+        CK(cons_sums(q, c->g.n, c->cons_part, c->sc->cons, c->s));
+    }
+    c->launches += 2;
+    return HC_OK;
+}
+
+extern "C" int hc_conservation_sums(hc_ctx *c, double *out)
+{
+    if (!c || !out) return set_err(HC_ERR_ARG, "null argument");
+    if (c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    CK(cudaSetDevice(c->dev));
+    int rc = launch_cons_sums(c);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->hsc->cons, c->sc->cons, sizeof c->hsc->cons, cudaMemcpyDeviceToHost, c->s));
+    rc = sync_ctx(c);
+    if (rc) return rc;
+    for (int v = 0; v < 5; v++) out[v] = c->hsc->cons[v];
+    return HC_OK;
+}
+
+extern "C" int hc_set_conservation_record(hc_ctx *c, int on)
+{
+    if (!c || (on != 0 && on != 1)) return set_err(HC_ERR_ARG, "bad argument");
+    if (c->cfg.gravity_only && on) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    c->cons_record = on;
+    return HC_OK;
 }
 
 extern "C" int hc_get_diag(hc_ctx *c, hc_diag *d)
@@ -1418,6 +1485,15 @@ extern "C" int hc_set_unet_passes(hc_ctx *c, int passes)
 {
     if (!c || passes < 1 || passes > 8) return set_err(HC_ERR_ARG, "passes must be 1..8");
     c->unet_passes = passes;
+    return HC_OK;
+}
+
+extern "C" int hc_set_unet_guard(hc_ctx *c, int consecutive_losses)
+{
+    if (!c || consecutive_losses < 0 || consecutive_losses > 64)
+        return set_err(HC_ERR_ARG, "consecutive_losses must be 0..64");
+    c->guard = UnetGuard();
+    c->guard.K = consecutive_losses;
     return HC_OK;
 }
 

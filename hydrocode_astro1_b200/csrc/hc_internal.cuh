@@ -4,7 +4,29 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/hydrocode_b200.h"
+
+namespace hc {
+
+// Raises a kernel's dynamic shared-memory limit once per device: `done` holds
+// one bit per device ordinal (below 64; beyond that the attribute is set on
+// every call).  Two threads may both set it the first time, which is harmless.
+inline cudaError_t set_smem_once(std::atomic<unsigned long long> &done, const void *fn, int bytes)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_release);
+    return e;
+}
+
+}  // namespace hc
+
 
 namespace hc {
 
@@ -38,6 +60,7 @@ struct DevScalars {
     unsigned long long resid_bits; // scratch
     double moments[4 + 9];        // M, COM, Q (reference mode)
     double resnorm;               // post-hoc residual
+    double cons[5];               // FP64 sums of rho, rho u, rho v, rho w, E
 };
 
 // Boundary-cell enumeration: index t in [0, nb) -> (i,j,k) on the faces.
@@ -109,6 +132,16 @@ cudaError_t ic_profile_stars(const Geom &g, double gamma, int nstars, const int 
                              double *scratch, cudaStream_t s);
 // opt-in MUSCL-Hancock interior update (FP64) -- hydro_plm.cu; pl: 20 n doubles of scratch
 cudaError_t fp64_plm_interior(const HydroArgs &a, double *pl, cudaStream_t s);
+
+// FP64 global sums of the 5 conserved fields (fixed order) -- conservation.cu.
+// partial: 5 * CONS_BLOCKS doubles of scratch; out: 5 doubles (device).
+constexpr int CONS_BLOCKS = 1184;
+template <typename T>
+struct ConsFields {
+    const T *f[5];
+};
+template <typename T>
+cudaError_t cons_sums(const ConsFields<T> &q, long long n, double *partial, double *out, cudaStream_t s);
 
 // FP32 hydro path -- hydro_fp32.cu
 cudaError_t fp32_cfl_full(const HydroArgs &a, cudaStream_t s);

@@ -8,7 +8,7 @@
 // also synchronise the whole device, which such a caller's other streams must
 // not see.  hc_sor_solve_noalloc therefore calls no cudaMalloc, cudaFree or
 // allocating library routine: the caller passes phi (in/out) and rho, and the
-// only scratch -- one residual slot per iteration plus two flags -- is the
+// only scratch -- one residual slot per iteration plus three words of flags -- is the
 // file-scope array below, a fixed 512 KB per GPU that loads the library,
 // held until the process exits.
 //
@@ -17,6 +17,8 @@
 // the same bit for bit.  The boundary cells of phi are kept as given.
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 
@@ -27,7 +29,9 @@ namespace {
 
 // Slot t (t < HC_NOALLOC_MAX_ITER) holds the bits of iteration t's max update;
 // [HC_NOALLOC_MAX_ITER] is the stop flag, [HC_NOALLOC_MAX_ITER + 1] the
-// iteration count at which the solve stopped.
+// iteration count at which the solve stopped, [HC_NOALLOC_MAX_ITER + 2] the
+// bits of the last executed iteration's update norm (written by check_kernel,
+// so the host reads flags and residual with one copy on the caller's stream).
 static __device__ __align__(256) unsigned long long g_sor_scratch[HC_NOALLOC_MAX_ITER + 8];
 
 struct Sor {
@@ -98,7 +102,15 @@ __global__ void __launch_bounds__(BX * BY) colour_kernel(Sor a, int color, int i
     }
 }
 
-__global__ void check_kernel(Sor a, int iter) { stop_here(a, iter); }
+// End of a batch of `iter` queued iterations: sets the stop flag if the last
+// one converged, then records the norm of the last iteration that ran.
+__global__ void check_kernel(Sor a, int iter)
+{
+    stop_here(a, iter);
+    const unsigned long long *flags = a.scr + HC_NOALLOC_MAX_ITER;
+    const int used = flags[0] ? (int)flags[1] : iter;
+    a.scr[HC_NOALLOC_MAX_ITER + 2] = a.scr[used - 1];
+}
 
 // Device address of the scratch array, looked up once per device with that
 // device current (in host code the symbol name is only a host-side stand-in).
@@ -116,6 +128,12 @@ cudaError_t scratch_for_current_device(unsigned long long **out)
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_sor_scratch);
         if (e != cudaSuccess) return e;
+        // load the three kernels now (lazy module loading would otherwise do
+        // it, and may allocate, at their first launch)
+        cudaFuncAttributes fa;
+        if ((e = cudaFuncGetAttributes(&fa, clear_kernel)) != cudaSuccess) return e;
+        if ((e = cudaFuncGetAttributes(&fa, colour_kernel)) != cudaSuccess) return e;
+        if ((e = cudaFuncGetAttributes(&fa, check_kernel)) != cudaSuccess) return e;
         g_scr_dev[dev] = static_cast<unsigned long long *>(p);
     }
     *out = g_scr_dev[dev];
@@ -125,6 +143,14 @@ cudaError_t scratch_for_current_device(unsigned long long **out)
 }  // namespace
 
 int hc_internal_set_error(int code, const char *msg);
+
+// HC_ERR_CUDA with `what` and the CUDA error's text as the message.
+static int cuda_fail(const char *what, cudaError_t e)
+{
+    char msg[256];
+    snprintf(msg, sizeof msg, "hc_sor_solve_noalloc: %s: %s", what, cudaGetErrorString(e));
+    return hc_internal_set_error(HC_ERR_CUDA, msg);
+}
 
 extern "C" int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int ny, int nz, double dx,
                                     double dy, double dz, double G, double omega, int max_iter,
@@ -138,6 +164,10 @@ extern "C" int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int 
                                                  "(the fixed scratch holds one slot per iteration)");
     if (!(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0))
         return hc_internal_set_error(HC_ERR_ARG, "hc_sor_solve_noalloc: cell sizes must be positive");
+    if (!(omega > 0.0 && omega < 2.0))
+        return hc_internal_set_error(HC_ERR_ARG, "hc_sor_solve_noalloc: omega must lie in (0, 2)");
+    if (!(tol > 0.0) || !std::isfinite(tol))
+        return hc_internal_set_error(HC_ERR_ARG, "hc_sor_solve_noalloc: tol must be finite and positive");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     Sor a;
     a.phi = phi;
@@ -151,14 +181,16 @@ extern "C" int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int 
     a.fac = 2.0 * (a.ix2 + a.iy2 + a.iz2);
     a.om = omega;
     a.tol = tol;
-    if (scratch_for_current_device(&a.scr) != cudaSuccess)
-        return hc_internal_set_error(HC_ERR_CUDA, "hc_sor_solve_noalloc: scratch address lookup failed");
+    cudaError_t e = scratch_for_current_device(&a.scr);
+    if (e != cudaSuccess)
+        return cuda_fail("scratch address lookup failed", e);
 
     clear_kernel<<<64, 256, 0, s>>>(a.scr, max_iter + 1);
     const dim3 grid(((nz - 1) / 2 + BX - 1) / BX, (ny - 2 + BY - 1) / BY, nx - 2);
     const dim3 block(BX, BY);
     int it = 0, batch = 16;
-    unsigned long long flags[2] = { 0ull, 0ull };
+    // stop flag, stopping iteration, bits of the last executed iteration's norm
+    unsigned long long flags[3] = { 0ull, 0ull, 0ull };
     while (true) {
         const int end = (max_iter - it < batch) ? max_iter : it + batch;
         for (int q = it; q < end; q++) {
@@ -166,21 +198,18 @@ extern "C" int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int 
             colour_kernel<<<grid, block, 0, s>>>(a, 1, q);
         }
         check_kernel<<<1, 1, 0, s>>>(a, end);
-        if (cudaGetLastError() != cudaSuccess)
-            return hc_internal_set_error(HC_ERR_CUDA, "hc_sor_solve_noalloc: kernel launch failed");
-        if (cudaMemcpyAsync(flags, a.scr + HC_NOALLOC_MAX_ITER, sizeof flags, cudaMemcpyDeviceToHost, s) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(s) != cudaSuccess)
-            return HC_ERR_CUDA;
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return cuda_fail("kernel launch failed", e);
+        if ((e = cudaMemcpyAsync(flags, a.scr + HC_NOALLOC_MAX_ITER, sizeof flags, cudaMemcpyDeviceToHost,
+                                 s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return cuda_fail("reading the stop flag failed", e);
         if (flags[0] || end >= max_iter) break;
         it = end;
         batch = batch < 256 ? 2 * batch : 256;
     }
     const int used = flags[0] ? (int)flags[1] : max_iter;
-    unsigned long long bits = 0ull;
-    if (cudaMemcpy(&bits, a.scr + (used - 1), sizeof bits, cudaMemcpyDeviceToHost) != cudaSuccess)
-        return HC_ERR_CUDA;
     if (iterations) *iterations = used;
-    if (residual) memcpy(residual, &bits, sizeof(double));
+    if (residual) memcpy(residual, &flags[2], sizeof(double));
     return flags[0] ? HC_OK : HC_NOT_CONVERGED;
 }

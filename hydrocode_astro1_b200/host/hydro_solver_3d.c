@@ -43,6 +43,7 @@ GodunovHLLC3D *solver3d_create(int nx, int ny, int nz, double xmin, double xmax,
     s->bc_xmin = s->bc_xmax = s->bc_ymin = s->bc_ymax = s->bc_zmin = s->bc_zmax = BC_OUTFLOW;
     s->log_every = 10;
     s->device_ics = -1;   /* profile set-ups on the device from 256^3 cells on */
+    s->unet_guard = 3;
     s->gravity_solver = NULL;
     if (s->enable_gravity) {
         s->gravity_solver = gravity_solver_create(nx, ny, nz, xmin, xmax, ymin, ymax, zmin, zmax, G);
@@ -101,6 +102,7 @@ GodunovHLLC3D *solver3d_create_from_deck(const InputDeck *d)   /* hydro_solver_3
     s->sor_depth = d->sor_depth;
     s->recon = d->recon;
     s->device_ics = d->device_ics;
+    s->unet_guard = d->unet_guard;
     s->max_steps = d->max_steps;
     s->log_every = d->log_every > 0 ? d->log_every : 10;
     strncpy(s->unet_weights, d->unet_weights, sizeof s->unet_weights - 1);
@@ -155,6 +157,8 @@ static int ensure_device(GodunovHLLC3D *s)
         if (hc_unet_load_file(s->dev, s->unet_weights) != HC_OK)
             fprintf(stderr, "Warning: learned warm start unavailable (%s); using the previous potential\n",
                     hc_last_error());
+        else if (s->unet_guard > 0 && hc_set_unet_guard(s->dev, s->unet_guard) != HC_OK)
+            fprintf(stderr, "Warning: learned-start monitor not set: %s\n", hc_last_error());
     }
     s->host_dirty = 1;
     return 0;

@@ -125,6 +125,7 @@ static const Field FIELDS[] = {
     F("log_normal_noise", K_DBL, log_noise), F("sor_depth", K_INT, sor_depth),
     F("checkpoint_every", K_INT, checkpoint_every), F("checkpoint_file", K_STR, checkpoint_file),
     F("reconstruction", K_RECON, recon), F("device_ics", K_INT, device_ics),
+    F("unet_guard", K_INT, unet_guard),
 };
 
 static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
@@ -175,6 +176,7 @@ static void set_defaults(InputDeck *d)   /* input_deck.c:63-153 */
     d->log_every = 10;
     strcpy(d->checkpoint_file, "checkpoint.ckpt");
     d->device_ics = -1;
+    d->unet_guard = 3;
 }
 
 static int is_true(const char *v) { return strcmp(v, "true") == 0 || strcmp(v, "1") == 0; }

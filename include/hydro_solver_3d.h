@@ -93,6 +93,7 @@ typedef struct GodunovHLLC3D {
     int device_ics;            /* profile-based set-ups built on the device: 1 always, 0 never,
                                   -1 (default) from 256^3 cells on */
     int ic_on_device;          /* the last set-up left the state on the device only */
+    int unet_guard;            /* learned-start outcome monitor: consecutive losses (0 = off) */
 } GodunovHLLC3D;
 
 GodunovHLLC3D *solver3d_create(int nx, int ny, int nz,

@@ -119,6 +119,15 @@ typedef struct hc_diag {
     long long unet_accepted; /* solves that started from the learned prediction */
     long long unet_fallbacks;/* solves whose prediction was rejected (larger FP64
                                 residual than the previous potential's) */
+    double cons[5];          /* with hc_set_conservation_record on: FP64 sums of
+                                rho, rho u, rho v, rho w, E over all cells after
+                                the last step of the last hc_step call */
+    /* learned-start outcome monitor (hc_set_unet_guard) */
+    long long unet_probes;   /* plain solves run to measure the network */
+    long long unet_wins;     /* comparisons the prediction won */
+    long long unet_losses;   /* comparisons it lost (no fewer iterations) */
+    long long unet_switch_offs;
+    int unet_off;            /* 1 while the network is switched off */
 } hc_diag;
 
 /* Per-kernel-family device time (CUDA events on the context's stream),
@@ -173,6 +182,19 @@ int hc_get_accel(hc_ctx *ctx, double *gx, double *gy, double *gz);
  * then 9 Cartesian Q (lmax == 0) or (lmax+1)^2 solid-harmonic moments. */
 int hc_get_moments(hc_ctx *ctx, double *mom, int cap);
 
+/* FP64 sums over all cells of the 5 conserved fields (rho, rho u, rho v,
+ * rho w, E; multiply by the cell volume for totals) of the device-resident
+ * state, in either precision, formed on the device in a fixed order (the same
+ * state gives the same bits) -- 40 bytes cross to the host, not the state.  No
+ * reference counterpart: the reference reports no totals, yet its step is not
+ * conservative (boundary cells are not flux-updated, hydro_solver_3d.c:729-731;
+ * the gravity source is not in flux form, :597-631; floors add mass,
+ * :765-768), so the drift of these sums measures a run's accuracy.
+ * hc_set_conservation_record(ctx, 1): every hc_step call also forms them after
+ * its last step and reports them in hc_diag.cons. */
+int hc_conservation_sums(hc_ctx *ctx, double *out5);
+int hc_set_conservation_record(hc_ctx *ctx, int on);
+
 /* FP64 max |(lap_nbrs(phi) - 4 pi G rho)/factor - phi| over the interior. */
 int hc_residual_norm(hc_ctx *ctx, double *out);
 
@@ -221,6 +243,22 @@ int hc_unet_loss_grad(hc_ctx *ctx, int nx, int ny, int nz, const float *x, const
 /* Predictions per solve (1..8, default 1): after an accepted prediction the
  * network is applied again to the residual it left, until one is rejected. */
 int hc_set_unet_passes(hc_ctx *ctx, int passes);
+/* Outcome monitor of the learned start (consecutive_losses K >= 1; 0, the
+ * default, turns it off).  The acceptance test of a prediction (max|delta|
+ * lower than the previous potential's) cannot see smooth error, so an
+ * accepted prediction may still cost SOR iterations.  The monitor compares
+ * the iterations of consecutive solves of which one started from a
+ * prediction and the other from the previous potential: a rejected
+ * prediction, or a plain "probe" solve it schedules after a number of
+ * predicted solves that grows with the network's advantage (64 solves and
+ * doubling to 1024 once a prediction needed under a quarter of the plain
+ * iterations; 16 under half; 4 otherwise; 2 after a loss).  After K
+ * consecutive losses the network is switched off, retried after 16 solves
+ * (doubling to 256 after each failed retry) and switched back on by a win.
+ * The first solve of a context is not compared.  Its state (counters in
+ * hc_diag) is not part of a checkpoint: a restarted run starts a fresh
+ * monitor.  No reference counterpart. */
+int hc_set_unet_guard(hc_ctx *ctx, int consecutive_losses);
 /* Correction cycles of a mixed-precision solve that start from a prediction
  * (1..8, default 2): the first from the step's residual, the second from the
  * smooth residual the first cycle's sweeps left; each prediction is kept only
@@ -298,16 +336,22 @@ int hc_unet_wgrad_test(int nx, int ny, int nz, const uint16_t *x, const uint16_t
  * rule are those of hc_gravity_solve (max |phi_GS - phi_old| < tol), so the
  * iterates match it bit for bit.  `stream` is a cudaStream_t (NULL: the
  * legacy default stream); the call returns after the solve has finished on
- * it.  Returns HC_OK, HC_NOT_CONVERGED, HC_ERR_ARG (max_iter outside
- * 1..HC_NOALLOC_MAX_ITER, a dimension below 3, null or non-positive inputs)
- * or HC_ERR_CUDA.
+ * it, having synchronised only that stream.  On HC_NOT_CONVERGED, iterations
+ * is max_iter and residual the last iteration's norm, as the context path
+ * reports them.  Returns HC_OK, HC_NOT_CONVERGED, HC_ERR_ARG (max_iter
+ * outside 1..HC_NOALLOC_MAX_ITER, a dimension below 3, null phi or rho,
+ * non-positive cell sizes, omega outside (0, 2), tol not finite and
+ * positive) or HC_ERR_CUDA (with hc_last_error() naming the failed call).
  *
  * Scratch: one residual slot per iteration plus two flags live in a fixed
  * file-scope device array of (HC_NOALLOC_MAX_ITER + 8) * 8 bytes (about
  * 512 KB) that every GPU loading this library holds until the process exits;
  * max_iter above HC_NOALLOC_MAX_ITER is rejected.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress) with that device
- * current: make that first call before any stream capture.  Every call shares
+ * current and loads the solver's kernels (with CUDA's lazy module loading that
+ * load would otherwise happen at their first launch, and loading a module may
+ * itself reserve device memory): make that first call at start-up, before any
+ * stream capture and before the caller's memory budget is fixed.  Every call shares
  * the array and clears what it needs at its start, so calls that overlap on
  * the GPU (concurrent streams, threads) race: serialise them. */
 #define HC_NOALLOC_MAX_ITER 65536

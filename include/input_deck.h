@@ -140,6 +140,8 @@ typedef struct {
     char checkpoint_file[256];  /* checkpoint_file (default checkpoint.ckpt; the latest one is kept) */
     int recon;                  /* reconstruction = constant | plm (MUSCL-Hancock, fp64 only) */
     int device_ics;             /* device_ics: profile set-ups on the device (1), host (0), auto (-1, default) */
+    int unet_guard;             /* unet_guard: learned-start outcome monitor, consecutive losses that
+                                   switch the network off (default 3; 0 = off) */
 } InputDeck;
 
 InputDeck *input_deck_create(const char *filename);

@@ -89,6 +89,7 @@ def test_gravity_polytrope_bitwise():
     assert_bitwise(s.state(), o.state(), "state")
     gx, gy, gz = s.accel()
     assert_bitwise(gx, o.gx, "gx")
+    assert_bitwise(gy, o.gy, "gy")
     assert_bitwise(gz, o.gz, "gz")
 
 

@@ -30,11 +30,15 @@ def noalloc_solve(phi_dev, rho_dev, shape, d, G, omega, max_iter, tol):
 
 
 @pytest.mark.skipif(not torch.cuda.is_available(), reason="no CUDA device")
-def test_noalloc_matches_context_solve_twice():
-    shape = (34, 30, 38)
+@pytest.mark.parametrize("shape,max_iter,expect", [
+    ((34, 30, 38), 20000, 0),      # even nz, converges
+    ((33, 31, 37), 20000, 0),      # odd sizes: the colour start k0 and the grid rounding along k
+    ((33, 31, 37), 7, -1),         # stops at max_iter: iterations and residual as the context reports them
+])
+def test_noalloc_matches_context_solve_twice(shape, max_iter, expect):
     lo, hi = (0.0, 0.0, 0.0), (1.0, 1.0, 1.0)
     d = tuple((hi[a] - lo[a]) / shape[a] for a in range(3))
-    G, omega, tol, max_iter = 1.0, 1.5, 1e-9, 20000
+    G, omega, tol = 1.0, 1.5, 1e-9
     q, _ = ics.polytrope_n1(shape, R=0.3)
     rho1 = q[0]
     rho2 = rho1 * (1.0 + 0.05 * np.cos(np.arange(rho1.size).reshape(shape) * 0.37))
@@ -56,7 +60,7 @@ def test_noalloc_matches_context_solve_twice():
 
         rc, it, res = noalloc_solve(phi_dev, rho_dev, shape, d, G, omega, max_iter, tol)
         torch.cuda.synchronize()
-        assert rc == rc_ref == hc.HC_OK, hc.last_error()
+        assert rc == rc_ref == expect, hc.last_error()
         assert it == ref_it and res == ref_res
         got = phi_dev.cpu().numpy()
         # FP64 with the same operation order: the tolerance of the FP64 parity
@@ -72,3 +76,7 @@ def test_noalloc_rejects_too_many_iterations():
     rho = torch.ones(shape, dtype=torch.float64, device="cuda")
     rc, _, _ = noalloc_solve(phi, rho, shape, (0.1, 0.1, 0.1), 1.0, 1.5, 65537, 1e-8)
     assert rc == -2 and "65536" in hc.last_error()
+    for om, tol in ((2.0, 1e-8), (0.0, 1e-8), (float("nan"), 1e-8), (1.5, float("nan")), (1.5, 0.0),
+                    (1.5, float("inf"))):
+        rc, _, _ = noalloc_solve(phi, rho, shape, (0.1, 0.1, 0.1), 1.0, om, 100, tol)
+        assert rc == -2, (om, tol)
