@@ -3,9 +3,12 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
+#include <cstring>
 
 #include "hydro_kernels.cuh"
+#include "hydro_fp32_pk.cuh"
 #include "hydro_fp32_tma.cuh"
 
 namespace hc {
@@ -49,8 +52,9 @@ cudaError_t fp32_dt(const HydroArgs &a, cudaStream_t s)
 }
 
 // TMA tensor map over the five FP32 fields of a state buffer:
-// dims (k, j, i, field), box (40, 10, 1, 5) -- one plane tile with halo.
-static cudaError_t encode_state_map(const HydroArgs &a, CUtensorMap *tm)
+// dims (k, j, i, field), box (40, 10, planes, 5) -- one (planes = 1) or two
+// (planes = 2) plane tiles with halo.
+static cudaError_t encode_state_map(const HydroArgs &a, CUtensorMap *tm, unsigned planes = 1)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     if (!enc) {
@@ -63,7 +67,7 @@ static cudaError_t encode_state_map(const HydroArgs &a, CUtensorMap *tm)
     const cuuint64_t n = (cuuint64_t)a.g.n;
     cuuint64_t dims[4] = { (cuuint64_t)a.g.nz, (cuuint64_t)a.g.ny, (cuuint64_t)a.g.nx, 5 };
     cuuint64_t strides[3] = { (cuuint64_t)a.g.nz * 4, (cuuint64_t)a.g.ny * a.g.nz * 4, n * 4 };
-    cuuint32_t box[4] = { (cuuint32_t)tma32::RK, (cuuint32_t)tma32::RJ, 1, 5 };
+    cuuint32_t box[4] = { (cuuint32_t)tma32::RK, (cuuint32_t)tma32::RJ, planes, 5 };
     cuuint32_t es[4] = { 1, 1, 1, 1 };
     CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(a.qin[0]), dims, strides, box,
                      es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -85,9 +89,80 @@ static bool tma_usable(const HydroArgs &a)
            ((uintptr_t)a.qin[0] % 16) == 0;
 }
 
+// Interior kernel: "pk" (default; packed FP32x2, two planes per thread),
+// "tma" (one plane per thread) or "plain" (no TMA), by HC_HYDRO32.
+static int hydro32_choice()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("HC_HYDRO32");
+        v = (e && !strcmp(e, "tma")) ? 1 : (e && !strcmp(e, "plain")) ? 2 : 0;
+    }
+    return v;
+}
+
+// Chunks along i for the packed kernel: the CTAs of all chunks run in waves
+// of `slots`; a chunk of L planes (L even) costs about L/2 + 1 plane-pair
+// steps (one for its prologue).  The chunk count minimising waves x steps.
+static int pk_chunks(long long tiles, int nint, long long slots)
+{
+    int best = 1;
+    double best_cost = 1e300;
+    const int max_ch = std::max(1, nint / 8);
+    for (int ch = 1; ch <= max_ch; ch++) {
+        int ilen = (nint + ch - 1) / ch;
+        ilen += ilen & 1;
+        const int n = (nint + ilen - 1) / ilen;
+        const long long waves = (tiles * n + slots - 1) / slots;
+        const double cost = (double)waves * (ilen / 2 + 1);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = n;
+        }
+    }
+    return best;
+}
+
+static cudaError_t pk_interior(const HydroArgs &a, cudaStream_t s)
+{
+    CUtensorMap tm;
+    cudaError_t e = encode_state_map(a, &tm, 2);
+    if (e != cudaSuccess) return e;
+    static std::atomic<unsigned long long> attr_set{0};
+    e = set_smem_once(attr_set, (const void *)pk::interior_pk_kernel, (int)pk::SMEM);
+    if (e != cudaSuccess) return e;
+    static int slots_dev[64] = { 0 };
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int slots = (dev >= 0 && dev < 64) ? slots_dev[dev] : 0;
+    if (!slots) {
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk::interior_pk_kernel, pk::NT, pk::SMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        slots = std::max(1, per_sm) * sms;
+        if (dev >= 0 && dev < 64) slots_dev[dev] = slots;
+    }
+    const long long tiles = (long long)((a.g.nz + pk::TK - 1) / pk::TK) * ((a.g.ny + pk::TJ - 1) / pk::TJ);
+    const int nint = a.g.nx - 2;
+    const int ch = pk_chunks(tiles, nint, slots);
+    int ilen = (nint + ch - 1) / ch;
+    ilen += ilen & 1;
+    const int n = (nint + ilen - 1) / ilen;
+    dim3 grid((a.g.nz + pk::TK - 1) / pk::TK, (a.g.ny + pk::TJ - 1) / pk::TJ, n);
+    pk::interior_pk_kernel<<<grid, dim3(pk::TK, pk::TJ), pk::SMEM, s>>>(tm, a, ilen);
+    return cudaGetLastError();
+}
+
 cudaError_t fp32_interior(const HydroArgs &a, int chunks, cudaStream_t s)
 {
-    if (tma_usable(a)) {
+    if (hydro32_choice() == 0 && tma_usable(a)) {
+        cudaError_t e = pk_interior(a, s);
+        if (e != cudaErrorInvalidValue) return e;   // the map could not be encoded: next kernel
+    }
+    if (hydro32_choice() <= 1 && tma_usable(a)) {
         CUtensorMap tm;
         cudaError_t e = encode_state_map(a, &tm);
         if (e == cudaSuccess) {
