@@ -491,6 +491,7 @@ static GravArgs grav_args(hc_ctx *c, const double *rho, const float *rho32)
     a.omega = c->cfg.omega;
     a.tol = c->cfg.tol;
     a.max_iter = c->cfg.max_iter;
+    a.sweep_kind = c->cfg.sor_depth == -3 ? 1 : 0;
     a.grav_bc = c->cfg.grav_bc;
     a.lmax = c->cfg.lmax;
     a.moment_order = c->cfg.moment_order;
@@ -700,12 +701,13 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
     // so a.omega here is theirs; the stopping test max|phi_GS - phi_old| < tol
     // does not depend on it
     if (c->corr_omega > 0.0) a.omega = c->corr_omega;
-    // sor_depth 0 (default): colour-split sweeps on e and r; -2: colour-split,
+    // sor_depth 0 (default): colour-split sweeps on e and r, staged by TMA
+    // where the layout allows (-3: the register vector sweeps); -2: colour-split,
     // two iterations per HBM pass (temporal blocking, out of place between
     // e32 and e32b; colour-split sweeps where the tiling does not fit); -1:
     // one in-place kernel per colour on the natural layout; >= 1: wavefront
     // passes of that many FP32 iterations per HBM pass on the natural layout
-    const bool split = (c->cfg.sor_depth == 0 || c->cfg.sor_depth == -2) && c->g.nz >= 3;
+    const bool split = (c->cfg.sor_depth == 0 || c->cfg.sor_depth == -2 || c->cfg.sor_depth == -3) && c->g.nz >= 3;
     const bool wave2 = split && c->cfg.sor_depth == -2 && mixed_wave_split_ok(c->g);
     const int depth = wave2 ? 2 : (split ? -1 : c->cfg.sor_depth);
     int rc = ensure_res(c, a.max_iter);

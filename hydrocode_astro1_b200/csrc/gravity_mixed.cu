@@ -16,7 +16,9 @@
 #include "hc_internal.cuh"
 #include "hc_math.cuh"
 #include "sor_split.cuh"
+#include "sor_split_tma.cuh"
 #include "sor_wave_split.cuh"
+#include "tmap.cuh"
 
 #ifndef HC_MIXED_PAIR
 #define HC_MIXED_PAIR 1   // pair forms of the FP64 residual / update where the layout allows
@@ -696,6 +698,47 @@ cudaError_t mixed_update(const GravArgs &a, const float *e32, bool split, float 
     return cudaGetLastError();
 }
 
+// TMA-staged colour sweep (sor_split_tma.cuh) when the rows fit one bulk
+// copy box and every stride is a multiple of 16 bytes; returns
+// cudaErrorNotSupported (nothing launched) otherwise.
+template <int NI, int NS>
+static cudaError_t sweep_tma(float *base, const float *src, const Split &sp, const SorCoef<float> &cf, int colour,
+                             double *res, int iter, double thresh, DevScalars *sc, cudaStream_t s)
+{
+    const size_t smem = (size_t)NS * stma::stage_floats<NI>(sp.H) * 4;
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = set_smem_once(attr_set, (const void *)stma::sor_split_tma_kernel<NI, NS>, (int)smem);
+    if (e != cudaSuccess) return e;
+    float *own = base + (size_t)colour * sp.cs;
+    const float *oth = base + (size_t)(colour ^ 1) * sp.cs;
+    const float *srcc = src + (size_t)colour * sp.cs;
+    CUtensorMap mo, mw, ms;
+    if (!tmap3(oth, 4, sp.nx, sp.ny, sp.H, sp.H, stma::TJ + 2, &mo, NI + 2) ||
+        !tmap3(own, 4, sp.nx, sp.ny, sp.H, sp.H, stma::TJ, &mw, NI) ||
+        !tmap3(srcc, 4, sp.nx, sp.ny, sp.H, sp.H, stma::TJ, &ms, NI))
+        return cudaErrorNotSupported;
+    stma::Tiles tl;
+    tl.nx = sp.nx;
+    tl.ny = sp.ny;
+    tl.nz = sp.nz;
+    tl.H = sp.H;
+    tl.ti = (sp.nx - 2 + NI - 1) / NI;
+    tl.tj = (sp.ny - 2 + stma::TJ - 1) / stma::TJ;
+    static int sms_dev[64] = { 0 };
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    int sms = (dev >= 0 && dev < 64) ? sms_dev[dev] : 0;
+    if (!sms) {
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) sms_dev[dev] = sms;
+    }
+    const int grid = std::min(tl.ti * tl.tj, sms);
+    return launch_pdl_smem(stma::sor_split_tma_kernel<NI, NS>, dim3(grid), dim3(stma::NT), smem, s, mo, mw, ms, own,
+                           tl, cf, colour, res, iter, thresh, sc);
+}
+
 cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, int colour, int iter,
                               double thresh, cudaStream_t s)
 {
@@ -705,7 +748,14 @@ cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, i
     cf.cy = mc.cy;
     cf.cz = mc.cz;
     cf.om = mc.om;
-    return launch_sor_split<float, float>(e32, r32, make_split(a.g), cf, colour, a.res, iter, thresh, a.sc, s);
+    const Split sp = make_split(a.g);
+    if (a.sweep_kind == 0 && sp.H % 4 == 0 && sp.H <= stma::HMAX && sp.nx >= 3 && sp.ny >= 3 &&
+        ((uintptr_t)e32 | (uintptr_t)r32) % 16 == 0 && sp.cs % 4 == 0) {
+        cudaError_t e = sp.H <= 128 ? sweep_tma<4, 2>(e32, r32, sp, cf, colour, a.res, iter, thresh, a.sc, s)
+                                    : sweep_tma<2, 2>(e32, r32, sp, cf, colour, a.res, iter, thresh, a.sc, s);
+        if (e != cudaErrorNotSupported) return e;
+    }
+    return launch_sor_split<float, float>(e32, r32, sp, cf, colour, a.res, iter, thresh, a.sc, s);
 }
 
 cudaError_t mixed_sor32(const GravArgs &a, float *e32, const float *r32, int color, int iter,
