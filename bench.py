@@ -66,6 +66,9 @@ def parse():
                     help="FP32 correction sweeps: 0 per-colour split sweeps, -2 two iterations per pass")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="skip the FP32 arm without the learned warm start")
+    ap.add_argument("--start-step", type=int, default=0,
+                    help="a late window: advance the workload this many steps (FP32 + learned start, untimed) "
+                         "and start every arm from that state")
     ap.add_argument("--record-fp64-iterations", default=None, metavar="PATH",
                     help="with --variant fp64: write the per-step SOR iteration counts to this JSON file "
                          "(the reference arm reads hydrocode_astro1_b200/data/fp64_iterations.json)")
@@ -196,6 +199,23 @@ def make_solver(p, variant, device):
         s.unet_passes(UNET_PASSES)
         s.unet_guard(UNET_GUARD)
     return s
+
+
+def advance(q0, p, nsteps, device):
+    """The workload's state after `nsteps` steps of the FP32 path with the
+    learned start (without it when no weight file exists), untimed: the
+    starting state of a late window.  Returns (state, time reached)."""
+    variant = "fp32_unet" if os.path.exists(UNET_WEIGHTS) else "fp32"
+    s = make_solver(p, variant, device)
+    s.set_state(q0)
+    t = 0.0
+    for k in range(nsteps):
+        t += float(s.step(1)[0])
+        if (k + 1) % 100 == 0:
+            log(f"[bench] advancing: step {k + 1} of {nsteps}, t = {t:.5f}")
+    q = s.state()
+    s.close()
+    return q, t
 
 
 def run_variant(q0, p, variant, steps, warmup, device, dist, clocks=None):
@@ -389,6 +409,9 @@ def main_ours(args):
         variant = "fp32_unet" if (args.n == 256 and os.path.exists(UNET_WEIGHTS)) else "fp32"
     q0, p = make_workload(args.n)
     ncell = p["shape"][0] * p["shape"][1] * p["shape"][2]
+    t_start = 0.0
+    if args.start_step > 0:
+        q0, t_start = advance(q0, p, args.start_step, local)
     clocks = Clocks(local)
     r = run_variant(q0, p, variant, args.steps, args.warmup, local, dist, clocks)
     ms = reduce_max(dist, r["ms"])
@@ -434,8 +457,10 @@ def main_ours(args):
         "dtype": "f64" if fp64 else ("f32 hydro / f64+f32 poisson / bf16 u-net" if variant == "fp32_unet"
                                      else "f32 hydro / f64+f32 poisson"),
         "data": "synthetic",
-        "config": {"workload": f"stellar_explosion_{args.n}^3 (n=3 star, lmax 8, tol 1e-8)",
+        "config": {"workload": f"stellar_explosion_{args.n}^3 (n=3 star, lmax 8, tol 1e-8)"
+                               + (f", window from step {args.start_step}" if args.start_step else ""),
                    "grid": list(p["shape"]), "variant": variant,
+                   "start_step": args.start_step, "t_start": t_start,
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (state >= 335 MB per buffer)"},
         "sor_iterations_per_step": r["iters"],
@@ -546,11 +571,13 @@ def main_ours(args):
             th, tit = reference_sample(q0, p, sor_iters=5)
             log(f"[bench] cpu baseline sample: hydro {th:.2f} s, SOR {tit * 1e3:.0f} ms/iteration "
                 f"({time.perf_counter() - t0:.1f} s total)")
+            # SOR iterations per step of the reference's algorithm: this run's
+            # FP64 arm when it ran, else the count recorded for the default window
             I = statistics.mean(r["iters"]) if fp64 else None
-            if I is None:
+            if I is None and "fp64_plain" in line:
+                I = statistics.mean(line["fp64_plain"]["sor_iterations_per_step"])
+            if I is None and args.start_step == 0:
                 I, _src = reference_iterations(args.n)
-                if I is None and "fp64_plain" in line:
-                    I = statistics.mean(line["fp64_plain"]["sor_iterations_per_step"])
             I = I or 1000.0
             t_step = th + I * tit
             line["cpu_baseline"] = {

@@ -1,18 +1,34 @@
-"""Accuracy report of the FP32 paths against the bit-exact FP64 path, per
-benchmark configuration.
+"""Per-configuration report: the FP32 paths against the FP64 path, at the
+configurations' stated run lengths.
 
     python -m hydrocode_astro1_b200.configs_report [--configs 0,1,2,3,4] [--out report.json]
+        [--arms fp64,fp32,fp32_unet] [--weights PATH ...] [--max-steps N]
 
 For each configuration the same initial state is stepped by the FP64 path
-(bit-identical to the reference C code, so it stands in for the FP64 oracle
-at these sizes) and by FP32 hydro + mixed-precision Poisson (and, where a
-trained network applies, with the learned warm start).  Reported per run:
-density L1 against FP64, relative mass and total-energy drift of each
-path, SOR iterations, and for the n=1 polytrope the central-density drift
-and the largest spurious speed; for the learned start the accepted and
-fallback counts.  Step counts are bounded so the whole report runs in a few
-minutes on one B200 (the long runs of the configurations -- t = 0.8,
-shock breakout, 2000 steps -- are not repeated here).
+(the reference's arithmetic and operation order in FP64; its l_max multipole
+moments in a fixed tree order) and by FP32 hydro + mixed-precision Poisson,
+without and with the learned warm start (one arm per weight file, each with
+the outcome monitor on).  Run lengths, as the configurations state them:
+
+  0  Sod 64^3                    to t = 0.2
+  1  n=1 polytrope 128^3         500 steps
+  2  cold collapse 192^3         to t = 0.8
+  3  stellar explosion 256^3     to shock breakout: the first step (checked
+                                 every 10) at which the cell of largest
+                                 rho * v_r (radial momentum density about the
+                                 star's centre) lies at r >= R; found by the
+                                 FP64 arm, the FP32 arms run its step count
+  4  two polytropes 512^3        2000 steps, FP32 arms; the FP64 arm runs the
+                                 first 20 steps (its full run takes hours) for
+                                 the density L1 at step 20
+
+Reported per arm: steps, time reached, wall time; SOR iterations per solve
+as per-100-step blocks (mean, median, 90th percentile); for the learned
+start the accepted and fallback counts per block and the monitor's counters;
+mass and total-energy drift from the FP64 totals each solver forms on the
+device (hc_conservation_sums); density L1 against the FP64 arm at the same
+step count; for the n=1 polytrope the central-density drift and the largest
+spurious speed.
 """
 from __future__ import annotations
 
@@ -30,16 +46,19 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import hydrocode_astro1_b200 as hc  # noqa: E402
 from hydrocode_astro1_b200 import problems  # noqa: E402
 
-WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "unet_stellar_explosion_256.bin")
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+WEIGHTS = os.path.join(DATA, "unet_stellar_explosion_256.bin")
+BLOCK = 100
 
-# configuration -> (name, builder, steps, t_end): run `steps` steps, or to t_end when given
+# configuration -> (name, builder, stop rule): ("steps", n) | ("t", t_end) | ("breakout", R)
 CONFIGS = {
-    0: ("sod_64", lambda: problems.sod_3d(64), None, 0.2),
-    1: ("polytrope_n1_128", lambda: problems.polytrope_n1(128), 100, None),
-    2: ("cold_collapse_192", lambda: problems.cold_collapse(192), 60, None),
-    3: ("stellar_explosion_256", lambda: problems.stellar_explosion(256), 30, None),
-    4: ("binary_n1_512", lambda: problems.binary_n1(512), 5, None),
+    0: ("sod_64", lambda: problems.sod_3d(64), ("t", 0.2)),
+    1: ("polytrope_n1_128", lambda: problems.polytrope_n1(128), ("steps", 500)),
+    2: ("cold_collapse_192", lambda: problems.cold_collapse(192), ("t", 0.8)),
+    3: ("stellar_explosion_256", lambda: problems.stellar_explosion(256), ("breakout", 0.4)),
+    4: ("binary_n1_512", lambda: problems.binary_n1(512), ("steps", 2000)),
 }
+FP64_STEPS_CAP = {4: 20}
 
 
 def solver(p, precision, warm=hc.HC_WARM_PREVIOUS):
@@ -48,64 +67,163 @@ def solver(p, precision, warm=hc.HC_WARM_PREVIOUS):
     return hc.HydroSolver3D(p["shape"], **kw)
 
 
-def run(q0, p, precision, steps, t_end, warm=hc.HC_WARM_PREVIOUS):
+def breakout_reached(q, p, R):
+    """The cell of largest radial momentum density rho v_r = m . r_hat (about
+    the origin, the star's centre) lies at r >= R."""
+    X, Y, Z = problems.centres(p["shape"], p["lo"], p["hi"])
+    r = np.sqrt(X * X + Y * Y + Z * Z)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        mr = (q[1] * X + q[2] * Y + q[3] * Z) / np.where(r > 0, r, 1.0)
+    i = np.unravel_index(np.argmax(mr), mr.shape)
+    return bool(r[i] >= R), float(r[i])
+
+
+def polytrope_figures(q0, q, p):
+    """Hydrostatic n=1 polytrope: drift of the central density and the
+    largest speed where the initial density exceeds 1e-3 of its maximum."""
+    ic = tuple(n // 2 for n in p["shape"])
+    star = q0[0] > 1e-3 * q0[0].max()
+    speed = np.sqrt((q[1:4] ** 2).sum(0)) / np.maximum(q[0], 1e-5)
+    return dict(central_density_drift=float(q[0][ic] / q0[0][ic] - 1), max_speed=float(speed[star].max()))
+
+
+def blocks(values, size=BLOCK):
+    out = []
+    for b in range(0, len(values), size):
+        v = np.asarray(values[b:b + size], dtype=float)
+        out.append(dict(steps=[b + 1, b + len(v)], mean=float(v.mean()), median=float(np.median(v)),
+                        p90=float(np.percentile(v, 90))))
+    return out
+
+
+def run(q0, p, precision, stop, warm=hc.HC_WARM_PREVIOUS, weights=None, max_steps=None, log=None, snap=None):
+    """Steps until the stop rule holds; returns the final state and the
+    record (with snap = k, also the density at step k as rec["_snap"])."""
+    kind, val = stop
     s = solver(p, precision, warm)
     if warm == hc.HC_WARM_UNET:
-        s.unet_load_file(WEIGHTS)
+        s.unet_load_file(weights)
+        s.unet_guard(3)
     s.set_state(q0)
-    t, n, iters = 0.0, 0, []
+    s.set_conservation_record(True)
+    c0 = s.conservation()
+    t, n, iters, acc, fb = 0.0, 0, [], [], []
+    breakout_r = None
+    snap_rho = None
     t0 = time.time()
-    while (t_end is None and n < steps) or (t_end is not None and t < t_end):
+    d_prev = s.diagnostics()
+    while True:
+        if kind == "steps" and n >= val:
+            break
+        if kind == "t" and t >= val:
+            break
+        if max_steps is not None and n >= max_steps:
+            break
         t += float(s.step(1)[0])
         n += 1
+        d = s.diagnostics()
         if p["G"] > 0:
-            iters.append(s.diagnostics()["last_iterations"])
+            iters.append(d["last_iterations"])
+            acc.append(d["unet_accepted"] - d_prev["unet_accepted"])
+            fb.append(d["unet_fallbacks"] - d_prev["unet_fallbacks"])
+        d_prev = d
+        if snap is not None and n == snap:
+            snap_rho = s.state()[0]
+        if kind == "breakout" and n % 10 == 0:
+            hit, rr = breakout_reached(s.state(), p, val)
+            if hit:
+                breakout_r = rr
+                break
+        if log and n % 100 == 0:
+            log(f"  step {n}, t {t:.5f}, {time.time() - t0:.0f} s")
+    c1 = np.array(d_prev["cons"]) if n > 0 else c0
     q = s.state()
     d = s.diagnostics()
     s.close()
-    return q, dict(steps=n, t=t, wall_s=time.time() - t0, sor_iterations=iters,
-                   unet_accepted=d["unet_accepted"], unet_fallbacks=d["unet_fallbacks"])
+    rec = dict(steps=n, t=t, wall_s=time.time() - t0,
+               mass_drift=float(c1[0] / c0[0] - 1.0), energy_drift=float(c1[4] / c0[4] - 1.0),
+               drift_source="hc_conservation_sums (FP64, on the device)")
+    if iters:
+        rec["sor_iterations_blocks"] = blocks(iters)
+        rec["sor_iterations_mean"] = float(np.mean(iters))
+        rec["sor_iterations_total"] = int(np.sum(iters))
+    if warm == hc.HC_WARM_UNET:
+        accb = [dict(steps=b["steps"], accepted=int(np.sum(acc[b["steps"][0] - 1:b["steps"][1]])),
+                     fallbacks=int(np.sum(fb[b["steps"][0] - 1:b["steps"][1]]))) for b in blocks(iters)]
+        rec.update(unet_accepted=d["unet_accepted"], unet_fallbacks=d["unet_fallbacks"],
+                   accepted_blocks=accb,
+                   monitor=dict(probes=d["unet_probes"], wins=d["unet_wins"], losses=d["unet_losses"],
+                                switch_offs=d["unet_switch_offs"], off_at_end=d["unet_off"]))
+    if breakout_r is not None:
+        rec["breakout_radius"] = breakout_r
+    if snap_rho is not None:
+        rec["_snap"] = snap_rho
+    return q, rec
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--configs", default="0,1,2,3,4")
+    ap.add_argument("--arms", default="fp64,fp32,fp32_unet")
+    ap.add_argument("--weights", nargs="*", default=None,
+                    help="weight files of the learned start (one fp32_unet arm each; default: the committed one)")
+    ap.add_argument("--max-steps", type=int, default=None, help="cap every run at this many steps")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
+    arms = a.arms.split(",")
+    weights = a.weights or [WEIGHTS]
+
+    def log(m):
+        print(m, file=sys.stderr, flush=True)
+
     out = []
     for c in [int(x) for x in a.configs.split(",")]:
-        name, build, steps, t_end = CONFIGS[c]
+        name, build, stop = CONFIGS[c]
         q0, p = build()
-        dV = np.prod([(p["hi"][t] - p["lo"][t]) / p["shape"][t] for t in range(3)])
-        m0, e0 = q0[0].sum() * dV, q0[4].sum() * dV
-        q64, r64 = run(q0, p, hc.FP64, steps, t_end)
-        arms = [("fp32", hc.HC_WARM_PREVIOUS)]
-        if p["G"] > 0 and all(n % 32 == 0 for n in p["shape"]) and os.path.exists(WEIGHTS):
-            arms.append(("fp32_unet", hc.HC_WARM_UNET))
-        rec = dict(config=c, name=name, shape=list(p["shape"]), fp64=dict(r64, mass_drift=float(q64[0].sum() * dV / m0 - 1),
-                                                                          energy_drift=float(q64[4].sum() * dV / e0 - 1)))
-        for arm, warm in arms:
-            q32, r32 = run(q0, p, hc.FP32, r64["steps"], None, warm)
-            rec[arm] = dict(r32, density_l1=float(np.abs(q32[0] - q64[0]).mean() / np.abs(q64[0]).mean()),
-                            mass_drift=float(q32[0].sum() * dV / m0 - 1),
-                            energy_drift=float(q32[4].sum() * dV / e0 - 1))
-            if warm == hc.HC_WARM_UNET:   # which network the learned-start figures belong to
-                with open(WEIGHTS, "rb") as f:
-                    rec[arm]["weights"] = dict(file=os.path.basename(WEIGHTS),
-                                               sha256=hashlib.sha256(f.read()).hexdigest()[:16])
-            if c == 1:   # hydrostatic n=1 polytrope: central density and spurious velocities
-                ic = tuple(n // 2 for n in p["shape"])
-                for tag, q in (("fp64", q64), (arm, q32)):
-                    rec[tag]["central_density_drift"] = float(q[0][ic] / q0[0][ic] - 1)
-                    rec[tag]["max_speed"] = float((np.sqrt((q[1:4] ** 2).sum(0)) / np.maximum(q[0], 1e-5))[
-                        q0[0] > 1e-3 * q0[0].max()].max())
-            del q32
+        rec = dict(config=c, name=name, shape=list(p["shape"]), stop=list(stop))
+        q64 = None
+        steps = None
+        if "fp64" in arms:
+            cap = FP64_STEPS_CAP.get(c, a.max_steps)
+            log(f"[{name}] fp64")
+            q64, r64 = run(q0, p, hc.FP64, stop, max_steps=cap, log=log)
+            if c == 1:
+                r64.update(polytrope_figures(q0, q64, p))
+            rec["fp64"] = r64
+            steps = r64["steps"]
+        fp32_stop = ("steps", steps) if (steps is not None and c not in FP64_STEPS_CAP) else stop
+        for arm in arms:
+            if arm == "fp64":
+                continue
+            unet = arm == "fp32_unet"
+            if unet and not (p["G"] > 0 and all(n % 32 == 0 for n in p["shape"])):
+                continue
+            for wf in (weights if unet else [None]):
+                tag = arm if not unet or len(weights) == 1 else f"{arm}:{os.path.basename(wf)}"
+                log(f"[{name}] {tag}")
+                snap = rec["fp64"]["steps"] if (q64 is not None and c in FP64_STEPS_CAP) else None
+                q32, r32 = run(q0, p, hc.FP32, fp32_stop, hc.HC_WARM_UNET if unet else hc.HC_WARM_PREVIOUS, wf,
+                               max_steps=a.max_steps, log=log, snap=snap)
+                rho_snap = r32.pop("_snap", None)
+                if q64 is not None and r32["steps"] == rec["fp64"]["steps"]:
+                    r32["density_l1"] = float(np.abs(q32[0] - q64[0]).mean() / np.abs(q64[0]).mean())
+                elif q64 is not None and rho_snap is not None:
+                    r32["density_l1"] = float(np.abs(rho_snap - q64[0]).mean() / np.abs(q64[0]).mean())
+                    r32["density_l1_at_step"] = snap
+                if unet:
+                    with open(wf, "rb") as f:
+                        r32["weights"] = dict(file=os.path.basename(wf),
+                                              sha256=hashlib.sha256(f.read()).hexdigest()[:16])
+                if c == 1:
+                    r32.update(polytrope_figures(q0, q32, p))
+                rec[tag] = r32
+                del q32
         print(json.dumps(rec), flush=True)
         out.append(rec)
         del q64
-    if a.out:
-        with open(a.out, "w") as f:
-            json.dump(out, f, indent=1)
+        if a.out:   # written after every configuration
+            with open(a.out, "w") as f:
+                json.dump(out, f, indent=1)
 
 
 if __name__ == "__main__":

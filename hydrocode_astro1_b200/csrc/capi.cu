@@ -110,7 +110,7 @@ struct hc_ctx {
     int debug;                   // HC_DEBUG=1: per-solve progress on stderr
     int unet_passes;             // learned-start predictions per solve (>= 1)
     int unet_cycles;             // correction cycles that start from a prediction (0: 2)
-    int unet_record_cycle;       // the cycle whose residual is recorded for training (0: 1)
+    int unet_record_cycle;       // the cycle whose residual is recorded for training (0: 1; -1: none)
     double corr_omega;           // relaxation of the FP32 correction sweeps (0: the solve's omega)
     UnetGuard guard;             // learned-start outcome monitor (hc_set_unet_guard)
     double *cons_part;           // conservation sums: 5 * CONS_BLOCKS block partials
@@ -751,7 +751,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         // With sample collection on, the residual and phi at the start of
         // cycle unet_record_cycle are recorded for training.
         const int ucycles = c->unet_cycles > 0 ? c->unet_cycles : 2;
-        const int rcycle = c->unet_record_cycle > 0 ? c->unet_record_cycle : 1;
+        const int rcycle = c->unet_record_cycle > 0 ? c->unet_record_cycle : (c->unet_record_cycle < 0 ? 0 : 1);
         if ((cycles <= ucycles || cycles == rcycle) && split && c->unet && std::isfinite(dmax)) {
             const bool predict = cycles <= ucycles && c->cfg.warm_start == HC_WARM_UNET && guard_ok &&
                                  unet_has_weights(c->unet);
@@ -1508,8 +1508,8 @@ extern "C" int hc_set_unet_cycles(hc_ctx *c, int cycles)
 
 extern "C" int hc_set_unet_record_cycle(hc_ctx *c, int cycle)
 {
-    if (!c || cycle < 1 || cycle > 8) return set_err(HC_ERR_ARG, "cycle must be 1..8");
-    c->unet_record_cycle = cycle;
+    if (!c || cycle < 0 || cycle > 8) return set_err(HC_ERR_ARG, "cycle must be 0..8");
+    c->unet_record_cycle = cycle == 0 ? -1 : cycle;   // -1: record nothing
     return HC_OK;
 }
 

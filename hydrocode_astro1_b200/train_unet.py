@@ -47,53 +47,98 @@ def solver(q, p, warm=hc.HC_WARM_PREVIOUS):
     return s
 
 
+def _list(v, n, cast):
+    parts = [cast(x) for x in str(v).split(",")]
+    if len(parts) == 1:
+        parts = parts * n
+    if len(parts) != n:
+        raise SystemExit(f"expected 1 or {n} comma-separated values, got {v}")
+    return parts
+
+
+def collect(problem, n, seed, solves, every, skip, cycles, init_seed):
+    """A plain-solver run of the problem that records `solves` samples per
+    recorded cycle, one every `every` solves after `skip` unrecorded ones."""
+    q, p = make(problem, n, seed)
+    s = solver(q, p)
+    s.unet_collect(solves * len(cycles) + 1)
+    s.unet_init(init_seed)
+    iters = []
+    for _ in range(skip):
+        s.unet_record_cycle(0)
+        s.step(1)
+        iters.append(s.diagnostics()["last_iterations"])
+    for c in cycles:
+        for _ in range(solves):
+            for k in range(every):
+                s.unet_record_cycle(c if k == every - 1 else 0)
+                s.step(1)
+                iters.append(s.diagnostics()["last_iterations"])
+    return s, iters
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--problem", default="stellar_explosion")
-    ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--seed", type=int, default=7)
-    ap.add_argument("--solves", type=int, default=25)
+    ap.add_argument("--problem", default="stellar_explosion",
+                    help="problem, or comma-separated problems trained on together")
+    ap.add_argument("--n", default="256", help="grid cells per side (one value, or one per problem)")
+    ap.add_argument("--seed", default="7", help="density-noise seed of the explosion (one, or per problem)")
+    ap.add_argument("--solves", default="25", help="samples per recorded cycle (one, or per problem)")
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--init-seed", type=int, default=1)
     ap.add_argument("--record-cycles", default="1",
                     help="correction cycles to record, `solves` steps each, in this order")
+    ap.add_argument("--record-every", default="1",
+                    help="record every k-th solve (k - 1 unrecorded steps between samples), so that "
+                         "`solves` samples span solves x k steps of the run (one, or per problem)")
+    ap.add_argument("--skip", default="0", help="unrecorded steps before the first sample (one, or per problem)")
     ap.add_argument("--out", required=True)
     a = ap.parse_args()
     t0 = time.time()
-    q, p = make(a.problem, a.n, a.seed)
-    s = solver(q, p)
+    probs = a.problem.split(",")
+    m = len(probs)
+    ns, seeds = _list(a.n, m, int), _list(a.seed, m, int)
+    solves, every, skip = _list(a.solves, m, int), _list(a.record_every, m, int), _list(a.skip, m, int)
     cycles = [int(c) for c in a.record_cycles.split(",")]
-    s.unet_collect(a.solves * len(cycles) + 1)
-    s.unet_init(a.init_seed)
-    iters = []
-    for c in cycles:
-        s.unet_record_cycle(c)
-        for _ in range(a.solves):
-            s.step(1)
-            iters.append(s.diagnostics()["last_iterations"])
+    runs = [collect(probs[q], ns[q], seeds[q], solves[q], every[q], skip[q], cycles, a.init_seed) for q in range(m)]
     t_collect = time.time() - t0
     losses = []
-    chunk = max(1, a.train_steps // 10)
-    # one cosine schedule over all steps, reported in ten chunks
+    nchunk = 10 * m
+    chunk = max(1, a.train_steps // nchunk)
+    # one linearly decaying learning rate over all steps, in chunks (each a
+    # cosine cycle); with several problems the chunks alternate between their
+    # sample rings, the parameters handed from one context to the next
     done = 0
     lr = a.lr
+    cur = 0
+    params = None
     while done < a.train_steps:
         k = min(chunk, a.train_steps - done)
+        s = runs[cur][0]
+        if params is not None and m > 1:
+            s.unet_load(params[0], params[1])
         losses.append(s.unet_train(k, lr=lr * (1.0 - done / a.train_steps), seed=1000 + done))
+        if m > 1:
+            params = s.unet_params()
         done += k
+        cur = (cur + 1) % m
     t_train = time.time() - t0 - t_collect
-    s.unet_save_file(a.out)
-    tm = s.timing()
-    report = {"problem": a.problem, "n": a.n, "seed": a.seed, "solves": a.solves, "record_cycles": cycles,
-              "samples": s.unet_samples(),
-              "sor_iterations": iters, "train_steps": a.train_steps, "lr": a.lr,
+    last = runs[(cur - 1) % m][0]
+    last.unet_save_file(a.out)
+    tm = last.timing()
+    report = {"problem": probs, "n": ns, "seed": seeds, "solves": solves, "record_cycles": cycles,
+              "record_every": every, "skip": skip,
+              "samples": [r[0].unet_samples() for r in runs],
+              "sor_iterations": [r[1] for r in runs], "train_steps": a.train_steps, "lr": a.lr,
+              "init_seed": a.init_seed,
               "loss_per_chunk": losses, "collect_s": t_collect, "train_s": t_train,
               "unet_device_ms": tm["unet_ms"], "params": hc.lib().hc_unet_param_count()}
     with open(os.path.splitext(a.out)[0] + ".json", "w") as f:
         json.dump(report, f, indent=1)
     print(json.dumps(report))
-    s.close()
+    for r in runs:
+        r[0].close()
 
 
 if __name__ == "__main__":

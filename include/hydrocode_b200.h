@@ -269,7 +269,8 @@ int hc_set_unet_guard(hc_ctx *ctx, int consecutive_losses);
  * if it lowers max|delta|. */
 int hc_set_unet_cycles(hc_ctx *ctx, int cycles);
 /* With collection on (hc_unet_collect): the correction cycle whose starting
- * residual is recorded as a training sample (1..8, default 1). */
+ * residual is recorded as a training sample (1..8, default 1; 0 records
+ * nothing, which pauses collection between the solves to be sampled). */
 int hc_set_unet_record_cycle(hc_ctx *ctx, int cycle);
 /* Relaxation factor of the FP32 correction sweeps of a mixed-precision solve
  * (0 < omega < 2; 0 restores the default, the solve's own omega).  No
