@@ -45,7 +45,7 @@ class Config(C.Structure):
         ("grav_bc", C.c_int), ("lmax", C.c_int), ("omega", C.c_double),
         ("tol", C.c_double), ("max_iter", C.c_int), ("sor_depth", C.c_int),
         ("warm_start", C.c_int), ("device", C.c_int), ("gravity_only", C.c_int),
-        ("recon", C.c_int),
+        ("recon", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
     ]
 
 
@@ -96,6 +96,9 @@ CAPI = {
     "hc_get_moments": (C.c_int, [C.c_void_p, _dp, C.c_int]),
     "hc_residual_norm": (C.c_int, [C.c_void_p, _dp]),
     "hc_conservation_sums": (C.c_int, [C.c_void_p, _dp]),
+    "hc_get_signal_speed": (C.c_int, [C.c_void_p, _dp]),
+    "hc_set_signal_speed": (C.c_int, [C.c_void_p, C.c_double]),
+    "hc_copy_planes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "hc_set_conservation_record": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_get_diag": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
     "hc_get_timing": (C.c_int, [C.c_void_p, C.POINTER(Timing), C.c_int]),
@@ -314,6 +317,22 @@ class HydroSolver3D:
         out = np.zeros(5)
         _check(self.L.hc_conservation_sums(self.h, _p(out)), "hc_conservation_sums")
         return out
+
+    # slabs of a larger grid ---------------------------------------------------
+    def signal_speed(self):
+        """The CFL maximum of |u_d| + c the next step's dt is formed from."""
+        v = C.c_double(0.0)
+        _check(self.L.hc_get_signal_speed(self.h, C.byref(v)), "hc_get_signal_speed")
+        return v.value
+
+    def set_signal_speed(self, s):
+        _check(self.L.hc_set_signal_speed(self.h, float(s)), "hc_set_signal_speed")
+
+    def copy_planes(self, i0, count, dev_ptr, to_ctx):
+        """Planes [i0, i0+count) of the 5 state fields to (to_ctx False) or
+        from (True) the device buffer at dev_ptr, field by field."""
+        _check(self.L.hc_copy_planes(self.h, int(i0), int(count), C.c_void_p(int(dev_ptr)), int(bool(to_ctx))),
+               "hc_copy_planes")
 
     def set_conservation_record(self, on=True):
         """Form the sums after every hc_step call (hc_diag 'cons')."""

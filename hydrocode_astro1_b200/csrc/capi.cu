@@ -321,9 +321,9 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
     g.nx = k.nx; g.ny = k.ny; g.nz = k.nz;
     g.n = (long long)k.nx * k.ny * k.nz;
     g.xmin = k.xmin; g.xmax = k.xmax; g.ymin = k.ymin; g.ymax = k.ymax; g.zmin = k.zmin; g.zmax = k.zmax;
-    g.dx = (k.xmax - k.xmin) / k.nx;
-    g.dy = (k.ymax - k.ymin) / k.ny;
-    g.dz = (k.zmax - k.zmin) / k.nz;
+    g.dx = k.dx > 0.0 ? k.dx : (k.xmax - k.xmin) / k.nx;
+    g.dy = k.dy > 0.0 ? k.dy : (k.ymax - k.ymin) / k.ny;
+    g.dz = k.dz > 0.0 ? k.dz : (k.zmax - k.zmin) / k.nz;
     c->gravity = k.G > 0.0;
     const size_t n = (size_t)g.n;
     int rc = HC_OK;
@@ -1358,6 +1358,79 @@ extern "C" int hc_timer_stop(hc_ctx *c, double *ms)
     CK(cudaEventElapsedTime(&f, c->t0, c->t1));
     *ms = f;
     c->timer_on = 0;
+    return sync_ctx(c);
+}
+
+// ---------------------------------------------------------------- slabs
+extern "C" int hc_get_signal_speed(hc_ctx *c, double *s)
+{
+    if (!c || !s) return set_err(HC_ERR_ARG, "null argument");
+    if (c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    CK(cudaSetDevice(c->dev));
+    const bool f64 = c->cfg.precision == HC_FP64;
+    if (!c->cfl_valid) {
+        HydroArgs a = hydro_args(c);
+        FamTimer t(c, FAM_BC);
+        CK(f64 ? fp64_cfl_full(a, c->s) : fp32_cfl_full(a, c->s));
+        c->launches += 2;
+        c->cfl_valid = 1;
+    }
+    CK(cudaMemcpyAsync(&c->hsc->smax[c->parity], &c->sc->smax[c->parity], sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, c->s));
+    int rc = sync_ctx(c);
+    if (rc) return rc;
+    const unsigned long long b = c->hsc->smax[c->parity];
+    double v;
+    if (f64) {
+        memcpy(&v, &b, sizeof v);
+    } else {
+        const unsigned int lo = (unsigned int)b;
+        float f;
+        memcpy(&f, &lo, sizeof f);
+        v = f;
+    }
+    *s = v;
+    return HC_OK;
+}
+
+extern "C" int hc_set_signal_speed(hc_ctx *c, double s)
+{
+    if (!c || !(s > 0.0) || !std::isfinite(s)) return set_err(HC_ERR_ARG, "signal speed must be finite and positive");
+    if (c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    CK(cudaSetDevice(c->dev));
+    unsigned long long b = 0;
+    if (c->cfg.precision == HC_FP64) {
+        memcpy(&b, &s, sizeof b);
+    } else {
+        const float f = (float)s;
+        if ((double)f != s) return set_err(HC_ERR_ARG, "FP32 context: the signal speed must be an FP32 value");
+        unsigned int lo;
+        memcpy(&lo, &f, sizeof lo);
+        b = lo;
+    }
+    c->hsc->smax[c->parity] = b;
+    CK(cudaMemcpyAsync(&c->sc->smax[c->parity], &c->hsc->smax[c->parity], sizeof b, cudaMemcpyHostToDevice, c->s));
+    c->cfl_valid = 1;
+    return sync_ctx(c);
+}
+
+extern "C" int hc_copy_planes(hc_ctx *c, int i0, int count, void *buf, int to_ctx)
+{
+    if (!c || !buf) return set_err(HC_ERR_ARG, "null argument");
+    if (c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context has no hydro state");
+    if (i0 < 0 || count < 0 || i0 + count > c->g.nx || (to_ctx != 0 && to_ctx != 1))
+        return set_err(HC_ERR_ARG, "planes [%d, %d) outside 0..%d", i0, i0 + count, c->g.nx);
+    CK(cudaSetDevice(c->dev));
+    const size_t word = c->cfg.precision == HC_FP64 ? 8 : 4;
+    const size_t plane = (size_t)c->g.ny * c->g.nz;
+    const size_t bytes = (size_t)count * plane * word;
+    for (int v = 0; v < 5; v++) {
+        char *field = c->cfg.precision == HC_FP64 ? reinterpret_cast<char *>(c->q64[c->cur][v])
+                                                  : reinterpret_cast<char *>(c->q32[c->cur][v]);
+        char *f = field + (size_t)i0 * plane * word;
+        char *b = static_cast<char *>(buf) + (size_t)v * bytes;
+        CK(cudaMemcpyAsync(to_ctx ? f : b, to_ctx ? b : f, bytes, cudaMemcpyDefault, c->s));
+    }
     return sync_ctx(c);
 }
 

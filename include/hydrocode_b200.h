@@ -108,6 +108,10 @@ typedef struct hc_config {
                                 (minmod-limited linear primitives with a half-step
                                 predictor), HC_FP64 only -- no reference
                                 counterpart */
+    double dx, dy, dz;       /* cell sizes; 0 (default): (max - min) / n as
+                                hydro_solver_3d.c:55-57.  A slab of a larger
+                                grid passes the whole grid's sizes so that its
+                                arithmetic is the whole grid's bit for bit */
 } hc_config;
 
 typedef struct hc_diag {
@@ -364,6 +368,23 @@ int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int ny, int nz,
                          double dx, double dy, double dz, double G, double omega,
                          int max_iter, double tol, void *stream,
                          int *iterations, double *residual);
+
+/* Slab decomposition support (no reference counterpart; the reference runs
+ * one grid in one process).  A grid split along i into slabs, one context per
+ * slab with a ghost plane on each side that has a neighbour, steps as the
+ * whole grid does when, between steps, (1) every slab's signal speed -- the
+ * CFL maximum of |u_d| + c over its cells that the next step's dt is formed
+ * from (hydro_solver_3d.c:422-450) -- is replaced by the maximum over the
+ * slabs, and (2) each ghost plane receives the neighbour's plane.
+ * hc_get_signal_speed forms it for a freshly set state; hc_set_signal_speed
+ * replaces it (a value another slab of the same precision produced).
+ * hc_copy_planes copies planes [i0, i0+count) of the 5 state fields to
+ * (to_ctx = 0) or from (to_ctx = 1) a device buffer laid out field by field
+ * (5 x count x ny x nz words of the context's precision).  Hydro only: with
+ * self-gravity (G > 0) the Poisson solve is not decomposed. */
+int hc_get_signal_speed(hc_ctx *ctx, double *s);
+int hc_set_signal_speed(hc_ctx *ctx, double s);
+int hc_copy_planes(hc_ctx *ctx, int i0, int count, void *dev_buf, int to_ctx);
 
 /* Page-lock (pin) a host buffer for faster transfers, and release it. */
 int hc_host_register(void *ptr, size_t bytes);

@@ -121,8 +121,8 @@ static cons_t hllc(cons_t qL, cons_t qR, int a, double gam)
     return f;
 }
 
-/* compute_dt_3d, hydro_solver_3d.c:422-450 */
-double hco_cfl_dt(hco_grid *g)
+/* The maximum signal speed of compute_dt_3d, hydro_solver_3d.c:422-442. */
+double hco_signal_max(const hco_grid *g)
 {
     double smax = 1.0e-10;
     size_t n = (size_t)g->nx * g->ny * g->nz;
@@ -133,6 +133,13 @@ double hco_cfl_dt(hco_grid *g)
         smax = mx(smax, fabs(w.v[1]) + cs);
         smax = mx(smax, fabs(w.v[2]) + cs);
     }
+    return smax;
+}
+
+/* compute_dt_3d, hydro_solver_3d.c:422-450 */
+double hco_cfl_dt(hco_grid *g)
+{
+    double smax = hco_signal_max(g);
     double tx = g->dx / smax, ty = g->dy / smax, tz = g->dz / smax;
     g->dt = g->cfl * mn(tx, mn(ty, tz));
     return g->dt;
@@ -698,7 +705,13 @@ static cons_t plm_flux(const hco_grid *g, const double *pl, size_t cl, size_t cr
     return hllc(cons_of_arr(L, g->gamma), cons_of_arr(R, g->gamma), a, g->gamma);
 }
 
-int hco_step(hco_grid *g)
+static int step_impl(hco_grid *g, double dt_given);
+
+int hco_step(hco_grid *g) { return step_impl(g, 0.0); }
+
+int hco_step_dt(hco_grid *g, double dt) { return step_impl(g, dt); }
+
+static int step_impl(hco_grid *g, double dt_given)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     const size_t n = (size_t)nx * ny * nz;
@@ -713,7 +726,8 @@ int hco_step(hco_grid *g)
         free(rho);
     }
 
-    hco_cfl_dt(g);
+    if (dt_given > 0.0) g->dt = dt_given;
+    else hco_cfl_dt(g);
     const double dt = g->dt, dx = g->dx, dy = g->dy, dz = g->dz;
 
     /* face fluxes F[a][c] = flux through the face between cell c and c+e_a,

@@ -47,6 +47,11 @@ int hco_step(hco_grid *g);
 
 /* compute_dt_3d (hydro_solver_3d.c:422-450): sets and returns g->dt. */
 double hco_cfl_dt(hco_grid *g);
+/* Its maximum signal speed max(|u_d| + c) over all cells (floor 1e-10). */
+double hco_signal_max(const hco_grid *g);
+/* One step with a given dt instead of the grid's own CFL dt: a slab of a
+ * larger grid steps with the whole grid's dt. */
+int hco_step_dt(hco_grid *g, double dt);
 
 /* gravity_solve / gravity_solve_potential / gravity_compute_acceleration
  * (gravity_solver_3d.c:905, :510, :753). */

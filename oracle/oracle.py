@@ -59,6 +59,10 @@ def oracle_lib():
         lib.hco_step.restype = C.c_int
         lib.hco_cfl_dt.argtypes = [gp]
         lib.hco_cfl_dt.restype = C.c_double
+        lib.hco_signal_max.argtypes = [gp]
+        lib.hco_signal_max.restype = C.c_double
+        lib.hco_step_dt.argtypes = [gp, C.c_double]
+        lib.hco_step_dt.restype = C.c_int
         lib.hco_gravity_solve.argtypes = [gp, _dp]
         lib.hco_gravity_solve.restype = C.c_int
         lib.hco_gravity_solve_potential.argtypes = [gp, _dp]
