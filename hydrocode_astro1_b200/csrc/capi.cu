@@ -44,9 +44,11 @@ static int set_err(int code, const char *fmt, ...)
 #define CK(call)                                                                         \
     do {                                                                                 \
         cudaError_t e_ = (call);                                                         \
-        if (e_ != cudaSuccess)                                                           \
+        if (e_ != cudaSuccess) {                                                         \
+            (void)cudaGetLastError(); /* a non-sticky error must not fail later calls */  \
             return set_err(HC_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,        \
                            cudaGetErrorString(e_));                                      \
+        }                                                                                \
     } while (0)
 
 extern "C" const char *hc_last_error(void) { return g_err; }
@@ -491,7 +493,7 @@ static GravArgs grav_args(hc_ctx *c, const double *rho, const float *rho32)
     a.omega = c->cfg.omega;
     a.tol = c->cfg.tol;
     a.max_iter = c->cfg.max_iter;
-    a.sweep_kind = c->cfg.sor_depth == -3 ? 1 : 0;
+    a.sweep_kind = c->cfg.sor_depth == -3 ? 1 : 0;   // 1: TMA-staged FP32 correction sweeps
     a.grav_bc = c->cfg.grav_bc;
     a.lmax = c->cfg.lmax;
     a.moment_order = c->cfg.moment_order;
@@ -701,8 +703,8 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
     // so a.omega here is theirs; the stopping test max|phi_GS - phi_old| < tol
     // does not depend on it
     if (c->corr_omega > 0.0) a.omega = c->corr_omega;
-    // sor_depth 0 (default): colour-split sweeps on e and r, staged by TMA
-    // where the layout allows (-3: the register vector sweeps); -2: colour-split,
+    // sor_depth 0 (default): colour-split sweeps on e and r (-3: the FP32
+    // correction sweeps staged by TMA where the layout allows); -2: colour-split,
     // two iterations per HBM pass (temporal blocking, out of place between
     // e32 and e32b; colour-split sweeps where the tiling does not fit); -1:
     // one in-place kernel per colour on the natural layout; >= 1: wavefront

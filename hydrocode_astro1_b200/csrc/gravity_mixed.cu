@@ -706,8 +706,12 @@ static cudaError_t sweep_tma(float *base, const float *src, const Split &sp, con
                              double *res, int iter, double thresh, DevScalars *sc, cudaStream_t s)
 {
     const size_t smem = (size_t)NS * stma::stage_floats<NI>(sp.H) * 4;
+    // the limit is raised once per device, to what the longest rows this
+    // instantiation takes need (HM cells per colour row)
+    constexpr int HM = NI == 4 ? 128 : stma::HMAX;
     static std::atomic<unsigned long long> attr_set{0};
-    cudaError_t e = set_smem_once(attr_set, (const void *)stma::sor_split_tma_kernel<NI, NS>, (int)smem);
+    cudaError_t e = set_smem_once(attr_set, (const void *)stma::sor_split_tma_kernel<NI, NS>,
+                                  (int)((size_t)NS * stma::stage_floats<NI>(HM) * 4));
     if (e != cudaSuccess) return e;
     float *own = base + (size_t)colour * sp.cs;
     const float *oth = base + (size_t)(colour ^ 1) * sp.cs;
@@ -749,7 +753,7 @@ cudaError_t mixed_sor32_split(const GravArgs &a, float *e32, const float *r32, i
     cf.cz = mc.cz;
     cf.om = mc.om;
     const Split sp = make_split(a.g);
-    if (a.sweep_kind == 0 && sp.H % 4 == 0 && sp.H <= stma::HMAX && sp.nx >= 3 && sp.ny >= 3 &&
+    if (a.sweep_kind == 1 && sp.H % 4 == 0 && sp.H <= stma::HMAX && sp.nx >= 3 && sp.ny >= 3 &&
         ((uintptr_t)e32 | (uintptr_t)r32) % 16 == 0 && sp.cs % 4 == 0) {
         cudaError_t e = sp.H <= 128 ? sweep_tma<4, 2>(e32, r32, sp, cf, colour, a.res, iter, thresh, a.sc, s)
                                     : sweep_tma<2, 2>(e32, r32, sp, cf, colour, a.res, iter, thresh, a.sc, s);

@@ -161,8 +161,8 @@ struct GravArgs {
     Geom g;
     double G, omega, tol;
     int max_iter;
-    int sweep_kind;           // FP32 correction colour sweeps: 0 TMA-staged where the layout
-                              // allows, 1 register vector sweeps
+    int sweep_kind;           // FP32 correction colour sweeps: 0 register vector sweeps,
+                              // 1 TMA-staged where the layout allows
     int grav_bc;
     int lmax;
     int moment_order;

@@ -89,11 +89,10 @@ typedef struct hc_config {
     double omega;            /* SOR relaxation (default 1.5) */
     double tol;              /* SOR tolerance on max |phi_GS - phi_old| */
     int max_iter;
-    int sor_depth;           /* SOR kernels: 0 (default) colour-split sweeps
-                                (the FP32 correction sweeps staged by TMA
-                                where rows of one colour hold at most 256
-                                cells, a multiple of 4); -3 colour-split with
-                                the FP32 correction sweeps in registers;
+    int sor_depth;           /* SOR kernels: 0 (default) colour-split sweeps;
+                                -3 colour-split with the FP32 correction
+                                sweeps staged by TMA where rows of one colour
+                                hold at most 256 cells, a multiple of 4;
                                 -2 colour-split, two FP32 correction
                                 iterations per HBM pass (temporal blocking);
                                 -1 natural-layout per-colour sweeps; >= 1

@@ -293,12 +293,12 @@ def test_fp32_3d_flow_close_to_fp64(shape):
 @pytest.mark.parametrize("shape", [(40, 37, 72), (130, 20, 32), (24, 60, 40), (70, 70, 64), (10, 12, 392),
                                    (21, 19, 38), (33, 31, 37)])
 def test_mixed_tma_sweeps_match_vector_sweeps(shape):
-    """The TMA-staged colour sweeps (the default, sor_depth 0: whole rows of
-    up to 256 cells per colour, row lengths a multiple of 4; plane tiles of 4,
-    or 2 for rows over 128 cells; partial tiles in i and j) give the register
-    vector sweeps' iterates (sor_depth -3) bit for bit after the same number
-    of correction iterations (shapes outside the TMA kernel's limits take the
-    vector or scalar sweeps in both runs)."""
+    """The TMA-staged colour sweeps (sor_depth -3: whole rows of up to 256
+    cells per colour, row lengths a multiple of 4; plane tiles of 4, or 2 for
+    rows over 128 cells; partial tiles in i and j) give the register vector
+    sweeps' iterates (the default, sor_depth 0) bit for bit after the same
+    number of correction iterations (shapes outside the TMA kernel's limits
+    take the vector or scalar sweeps in both runs)."""
     q0, gam = ics.polytrope_n1(shape, R=0.3)
     phis, norms = [], []
     for depth in (0, -3):
