@@ -25,6 +25,9 @@
 #ifndef HC_CYCLE_REDUCTION
 #define HC_CYCLE_REDUCTION 1.0e-4   // residual reduction a correction cycle's sweeps aim for
 #endif
+#ifndef HC_LAST_CYCLE_TARGET
+#define HC_LAST_CYCLE_TARGET 0.95   // the last cycle's sweeps stop below this fraction of tol
+#endif
 
 using namespace hc;
 
@@ -811,9 +814,11 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
         // one cycle reduces the residual 1e4-fold at most: FP32 resolves the
         // correction e to ~1e-7 |e|, and |e| can exceed max|delta| by the
         // grid's condition number on a cold start.  In the last cycle the
-        // sweeps run to the reference's own test: a red-black sweep whose
-        // update norm max |phi_GS - phi_old| is below tol.
-        const double thresh = std::max(a.tol, HC_CYCLE_REDUCTION * dmax);
+        // sweeps run to the reference's own test -- a red-black sweep whose
+        // update norm max |phi_GS - phi_old| is below tol -- with a margin
+        // for the FP32 rounding of that norm (checked below): to 0.95 tol.
+        const double tol_last = a.tol * HC_LAST_CYCLE_TARGET;
+        const double thresh = std::max(tol_last, HC_CYCLE_REDUCTION * dmax);
         const int budget = a.max_iter - total;
         CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));
         CK(grav_reset_slots(a, 0, budget + 8, c->s));
@@ -896,10 +901,15 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
             c->launches++;
         }
         // Converged by the reference's criterion when the last sweep's update
-        // norm (on e, which equals that of phi + e) is below tol and FP32
-        // resolves e finely enough that an update of size tol cannot round
-        // away: max|e| 2^-22 < tol.
-        if (done && thresh == a.tol) {
+        // norm (on e, which equals that of phi + e in exact arithmetic) is
+        // below tol with room for its FP32 rounding -- the FP32 Gauss-Seidel
+        // value of a cell sums its six neighbours' e (weights adding up to 1)
+        // and delta, so it is off from the FP64 one by a few units in the
+        // last place of max|e|; 4 ulp are allowed -- and FP32 resolves e
+        // finely enough that an update of size tol cannot round away:
+        // max|e| 2^-22 < tol.  Otherwise another correction cycle starts
+        // from the FP64 residual of the updated potential.
+        if (done && thresh == tol_last) {
             double snorm = 0.0;
             CK(cudaMemcpyAsync(&c->hsc->resnorm, c->res + (last - 1), sizeof(double), cudaMemcpyDeviceToHost,
                                c->s));
@@ -913,7 +923,7 @@ int hc_sor_mixed(hc_ctx *c, const float *rho32)
             if (c->debug)
                 fprintf(stderr, "[hc] mixed cycle %d: sweep norm %.3e, max|e| %.3e after %d sweeps\n", cycles, snorm,
                         emax, total);
-            if (snorm < a.tol && emax * 0x1p-22 < a.tol) {
+            if (snorm + 4.0 * emax * 0x1p-23 < a.tol && emax * 0x1p-22 < a.tol) {
                 dmax = snorm;
                 status = 0;
                 break;

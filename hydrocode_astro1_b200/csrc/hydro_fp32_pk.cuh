@@ -61,33 +61,13 @@ constexpr size_t OFF_WMAX = OFF_BAR + 16;
 constexpr size_t SMEM = OFF_WMAX + (NT / 32) * 4;
 
 // ---------------------------------------------------------------- packed arithmetic
-__device__ __forceinline__ unsigned long long b64(float2 a) { return *reinterpret_cast<unsigned long long *>(&a); }
-__device__ __forceinline__ float2 f64b(unsigned long long r) { return *reinterpret_cast<float2 *>(&r); }
-
-__device__ __forceinline__ float2 add2(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(b64(a)), "l"(b64(b)));
-    return f64b(r);
-}
-__device__ __forceinline__ float2 sub2(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(b64(a)), "l"(b64(b)));
-    return f64b(r);
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b)
-{
-    unsigned long long r;
-    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(b64(a)), "l"(b64(b)));
-    return f64b(r);
-}
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
-{
-    unsigned long long r;
-    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(b64(a)), "l"(b64(b)), "l"(b64(c)));
-    return f64b(r);
-}
+// sm_100 packed FP32x2 operations (CUDA's __fadd2_rn / __fmul2_rn / __ffma2_rn
+// intrinsics, which leave the register pairing to the compiler); a - b is
+// the fused b * (-1) + a, rounded once like a subtraction.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 sp2(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float2 max2(float2 a, float2 b) { return make_float2(tmax(a.x, b.x), tmax(a.y, b.y)); }
 __device__ __forceinline__ float2 min2(float2 a, float2 b) { return make_float2(tmin(a.x, b.x), tmin(a.y, b.y)); }
@@ -314,14 +294,20 @@ interior_pk_kernel(const __grid_constant__ CUtensorMap tmap, HydroArgs a, int il
         ok = mbar_wait(&bar[b], use[b] & 1) && ok;
         use[b]++;
     };
+    // the NH halo records are formed by threads HB .. HB+NH-1 (warps 3-5),
+    // the faces behind the tile by warps 6 and 7: the extra work of a step
+    // spread over warps that the barriers would otherwise hold up
+    constexpr int HB = 96;
+    static_assert(HB + NH <= 6 * 32, "halo records fit warps 3-5");
     auto build_halo = [&](const float *r) {
-        if (tid < NH) {
+        const int h = tid - HB;
+        if (h >= 0 && h < NH) {
             int sj, sk;
-            if (tid < 2 * SK) {
-                sj = (tid < SK) ? 0 : SJ - 1;
-                sk = tid % SK;
+            if (h < 2 * SK) {
+                sj = (h < SK) ? 0 : SJ - 1;
+                sk = h % SK;
             } else {
-                const int q = tid - 2 * SK;
+                const int q = h - 2 * SK;
                 sj = 1 + (q >> 1);
                 sk = (q & 1) ? SK - 1 : 0;
             }
@@ -368,9 +354,9 @@ interior_pk_kernel(const __grid_constant__ CUtensorMap tmap, HydroArgs a, int il
         // y and z faces ahead of the cell, and the CTA's faces behind the tile
         put_flux(FYa, FYb, FYe, (ty + 1) * TK + tx, hllc2<1>(C, get_rec(P, (ty + 2) * SK + tx + 1)));
         put_flux(FZa, FZb, FZe, ty * (TK + 1) + tx + 1, hllc2<2>(C, get_rec(P, own_s + 1)));
-        if (ty == 0) {
-            put_flux(FYa, FYb, FYe, tx, hllc2<1>(get_rec(P, tx + 1), C));
-        } else if (ty == 1 && tx < TJ) {
+        if (ty == TJ - 1) {          // the y faces below the tile's first row
+            put_flux(FYa, FYb, FYe, tx, hllc2<1>(get_rec(P, tx + 1), get_rec(P, SK + tx + 1)));
+        } else if (ty == TJ - 2 && tx < TJ) {   // the z faces before the tile's first column
             put_flux(FZa, FZb, FZe, tx * (TK + 1),
                      hllc2<2>(get_rec(P, (tx + 1) * SK), get_rec(P, (tx + 1) * SK + 1)));
         }
