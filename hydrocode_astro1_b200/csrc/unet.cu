@@ -168,6 +168,7 @@ struct UNetState {
     __nv_bfloat16 *ga[NLEV + 1], *gb[NLEV + 1], *gc[NLEV + 1];
     float *out0 = nullptr, *pooled = nullptr, *xnorm = nullptr, *partial = nullptr, *bpart = nullptr;
     double *scal = nullptr;       // [0] sumsq of the input, [1] sum t^2, [2] loss
+    double *rpart = nullptr;      // per-block partial sums of the input's squares (NRPART)
     int *err = nullptr;
     void *act_mem = nullptr;
     // training samples: normalised inputs and targets at level 0
@@ -188,6 +189,7 @@ int dalloc(void **p, size_t bytes)
     }
     return HC_OK;
 }
+constexpr int NRPART = 148 * 16;   // the most blocks nblk() gives
 inline unsigned nblk(long long n, int nt = 256)
 {
     long long b = (n + nt - 1) / nt;
@@ -266,7 +268,7 @@ int ensure_grid(UNetState *u, int gx, int gy, int gz)
         nbf += (size_t)u->L[l].n * CH * (l == 0 ? 8 : 7);
     }
     const size_t nf = 3 * (size_t)u->L[0].n + (size_t)MAX_PARTS * WG_MT * TM * CH + 148 * 16 * CH;
-    const size_t bytes = nbf * 2 + nf * 4 + 4 * sizeof(double) + 256 * 4;
+    const size_t bytes = nbf * 2 + nf * 4 + (4 + NRPART) * sizeof(double) + 256 * 4;
     if (dalloc(&u->act_mem, bytes)) return HC_ERR_NOMEM;
     char *p = (char *)u->act_mem;
     auto take_bf = [&](size_t n) { __nv_bfloat16 *r = (__nv_bfloat16 *)p; p += n * 2; return r; };
@@ -287,6 +289,7 @@ int ensure_grid(UNetState *u, int gx, int gy, int gz)
     u->bpart = take_f(148 * 16 * CH);
     p = (char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
     u->scal = (double *)p; p += 4 * sizeof(double);
+    u->rpart = (double *)p; p += NRPART * sizeof(double);
     u->err = (int *)p;
     u->gx = gx; u->gy = gy; u->gz = gz;
     // samples of another grid size are dropped
@@ -508,8 +511,9 @@ int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e
     int rc = ensure_grid(u, a.g.nx, a.g.ny, a.g.nz);
     if (rc) return rc;
     const Split sp = make_split(a.g);
-    cudaMemsetAsync(u->scal, 0, sizeof(double), s);
-    in_pool_kernel<<<nblk(u->L[0].n), 256, 0, s>>>(r32, sp, u->L[0], u->pooled, u->scal);
+    const unsigned npool = nblk(u->L[0].n);
+    in_pool_kernel<<<npool, 256, 0, s>>>(r32, sp, u->L[0], u->pooled, u->rpart);
+    sum_parts_kernel<<<1, 32, 0, s>>>(u->rpart, (int)npool, u->scal);
     const bool collect = record && u->cap > 0 && u->sx;
     u->slot = collect ? u->next : -1;
     float *xs = collect ? u->sx + (size_t)u->slot * u->L[0].n : nullptr;

@@ -196,9 +196,13 @@ __global__ void sum_partials_kernel(const float *__restrict__ partial, int npart
 // ---------------------------------------------------------------- solver side
 // pooled[v0] = average of the 8 grid cells of net voxel v0 of the residual
 // (colour-split FP32, zero on boundary cells); sumsq += pooled^2
+// The sum of squares goes to one partial per block (part[blockIdx.x]; 256
+// threads), added in a fixed order by sum_parts_kernel: the same input gives
+// the same bits (no atomics on one address).
 __global__ void in_pool_kernel(const float *__restrict__ r32, Split sp, Dims d0, float *__restrict__ pooled,
-                               double *__restrict__ sumsq)
+                               double *__restrict__ part)
 {
+    __shared__ double ws[8];
     double local = 0.0;
     UNET_LOOP(d0.n)
     {
@@ -215,7 +219,23 @@ __global__ void in_pool_kernel(const float *__restrict__ r32, Split sp, Dims d0,
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xffffffffu, local, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(sumsq, local);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) b += ws[w];
+        part[blockIdx.x] = b;
+    }
+}
+
+// out = sum of part[0..n) in a fixed order (one warp)
+__global__ void sum_parts_kernel(const double *__restrict__ part, int n, double *__restrict__ out)
+{
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < n; b += 32) acc += part[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) *out = acc;
 }
 
 // x0 (16 channels, channel 0 = pooled / rms, others 0)
@@ -269,8 +289,9 @@ __device__ __forceinline__ void lin_coarse(int i, int n0, int &a, int &b, float 
 // fixed, and thread m writes the cells k = 2m (colour (i+j)&1) and k = 2m+1
 // (the other colour), both at index m of their colour array.  Their k
 // neighbours in the coarse rows are columns m-1, m (k = 2m, weight 0.75 on m)
-// and m, m+1 (k = 2m+1, weight 0.25 on m+1), clamped at the ends: twelve
-// loads serve both cells, each formed in the order k, then j, then i.
+// and m, m+1 (k = 2m+1, weight 0.25 on m+1), clamped at the ends: each lane
+// loads column m of the four coarse rows and takes m-1 and m+1 from its
+// neighbour lanes; both cells are formed in the order k, then j, then i.
 constexpr int OUT_UP_ROWS = 16;
 __global__ void out_up_kernel(const float *__restrict__ out0, Dims d0, const double *__restrict__ sumsq, float kscale,
                               Split sp, float *__restrict__ e)
@@ -292,16 +313,30 @@ __global__ void out_up_kernel(const float *__restrict__ out0, Dims d0, const dou
         const float *p10 = out0 + vidx(d0, ib, ja, 0), *p11 = out0 + vidx(d0, ib, jb, 0);
         const int cc = (i + j) & 1;   // colour of k = 2m
         float *e0 = e + cc * sp.cs + row * sp.H, *e1 = e + (cc ^ 1) * sp.cs + row * sp.H;
-        for (int m = threadIdx.x; m < sp.H; m += blockDim.x) {
+        // whole warps run every pass (lanes past the row end hold the clamped
+        // last coarse values), so the coarse neighbours m-1 and m+1 come from
+        // the adjacent lanes; the lanes at a warp's edges load them
+        const int lane = threadIdx.x & 31;
+        const int Hw = (sp.H + 31) & ~31;
+        for (int m = threadIdx.x; m < Hw; m += blockDim.x) {
+            const int mc = min(m, n0 - 1);
+            const int km = max(m - 1, 0), kp = min(m + 1, n0 - 1);
+            const float b00 = p00[mc], b01 = p01[mc], b10 = p10[mc], b11 = p11[mc];
+            float a00 = __shfl_up_sync(0xffffffffu, b00, 1), a01 = __shfl_up_sync(0xffffffffu, b01, 1);
+            float a10 = __shfl_up_sync(0xffffffffu, b10, 1), a11 = __shfl_up_sync(0xffffffffu, b11, 1);
+            float c00 = __shfl_down_sync(0xffffffffu, b00, 1), c01 = __shfl_down_sync(0xffffffffu, b01, 1);
+            float c10 = __shfl_down_sync(0xffffffffu, b10, 1), c11 = __shfl_down_sync(0xffffffffu, b11, 1);
+            if (lane == 0 || m == 0) {
+                a00 = p00[km]; a01 = p01[km]; a10 = p10[km]; a11 = p11[km];
+            }
+            if (lane == 31 || m + 1 >= n0) {
+                c00 = p00[kp]; c01 = p01[kp]; c10 = p10[kp]; c11 = p11[kp];
+            }
+            if (m >= sp.H) continue;
             const int k0 = 2 * m, k1 = 2 * m + 1;
             const bool in0 = rin && k0 >= 1 && k0 <= sp.nz - 2, in1 = rin && k1 >= 1 && k1 <= sp.nz - 2;
             float v0 = 0.f, v1 = 0.f;
             if (in0 || in1) {
-                const int km = max(m - 1, 0), kp = min(m + 1, n0 - 1);
-                const float a00 = p00[km], b00 = p00[m], c00 = p00[kp];
-                const float a01 = p01[km], b01 = p01[m], c01 = p01[kp];
-                const float a10 = p10[km], b10 = p10[m], c10 = p10[kp];
-                const float a11 = p11[km], b11 = p11[m], c11 = p11[kp];
                 if (in0) {   // lin_coarse(2m): (m-1, m), weight 0.75 on m
                     const float wk = 0.75f;
                     const float s00 = a00 * (1.f - wk) + b00 * wk, s01 = a01 * (1.f - wk) + b01 * wk;
