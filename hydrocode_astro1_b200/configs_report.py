@@ -14,10 +14,12 @@ the outcome monitor on).  Run lengths, as the configurations state them:
   1  n=1 polytrope 128^3         500 steps
   2  cold collapse 192^3         to t = 0.8
   3  stellar explosion 256^3     to shock breakout: the first step (checked
-                                 every 10) at which the cell of largest
+                                 every 50) at which the cell of largest
                                  rho * v_r (radial momentum density about the
                                  star's centre) lies at r >= R; found by the
                                  FP64 arm, the FP32 arms run its step count
+                                 (with --fp64-steps N the FP64 arm stops at N
+                                 and each FP32 arm finds breakout itself)
   4  two polytropes 512^3        2000 steps, FP32 arms; the FP64 arm runs the
                                  first 20 steps (its full run takes hours) for
                                  the density L1 at step 20
@@ -49,6 +51,7 @@ from hydrocode_astro1_b200 import problems  # noqa: E402
 DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 WEIGHTS = os.path.join(DATA, "unet_stellar_explosion_256.bin")
 BLOCK = 100
+BREAKOUT_EVERY = 50
 
 # configuration -> (name, builder, stop rule): ("steps", n) | ("t", t_end) | ("breakout", R)
 CONFIGS = {
@@ -129,7 +132,7 @@ def run(q0, p, precision, stop, warm=hc.HC_WARM_PREVIOUS, weights=None, max_step
         d_prev = d
         if snap is not None and n == snap:
             snap_rho = s.state()[0]
-        if kind == "breakout" and n % 10 == 0:
+        if kind == "breakout" and n % BREAKOUT_EVERY == 0:
             hit, rr = breakout_reached(s.state(), p, val)
             if hit:
                 breakout_r = rr
@@ -168,6 +171,9 @@ def main():
     ap.add_argument("--weights", nargs="*", default=None,
                     help="weight files of the learned start (one fp32_unet arm each; default: the committed one)")
     ap.add_argument("--max-steps", type=int, default=None, help="cap every run at this many steps")
+    ap.add_argument("--fp64-steps", type=int, default=None,
+                    help="cap the FP64 arm at this many steps (the FP32 arms then run their own stop rule and "
+                         "the density L1 is taken at that step)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
     arms = a.arms.split(",")
@@ -177,6 +183,12 @@ def main():
         print(m, file=sys.stderr, flush=True)
 
     out = []
+
+    def save(recs):   # after every arm: a long run that is cut short keeps what it finished
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(recs, f, indent=1)
+
     for c in [int(x) for x in a.configs.split(",")]:
         name, build, stop = CONFIGS[c]
         q0, p = build()
@@ -184,14 +196,16 @@ def main():
         q64 = None
         steps = None
         if "fp64" in arms:
-            cap = FP64_STEPS_CAP.get(c, a.max_steps)
+            cap = a.fp64_steps or FP64_STEPS_CAP.get(c, a.max_steps)
             log(f"[{name}] fp64")
             q64, r64 = run(q0, p, hc.FP64, stop, max_steps=cap, log=log)
             if c == 1:
                 r64.update(polytrope_figures(q0, q64, p))
             rec["fp64"] = r64
             steps = r64["steps"]
-        fp32_stop = ("steps", steps) if (steps is not None and c not in FP64_STEPS_CAP) else stop
+            save(out + [rec])
+        capped = c in FP64_STEPS_CAP or a.fp64_steps is not None
+        fp32_stop = ("steps", steps) if (steps is not None and not capped) else stop
         for arm in arms:
             if arm == "fp64":
                 continue
@@ -201,7 +215,7 @@ def main():
             for wf in (weights if unet else [None]):
                 tag = arm if not unet or len(weights) == 1 else f"{arm}:{os.path.basename(wf)}"
                 log(f"[{name}] {tag}")
-                snap = rec["fp64"]["steps"] if (q64 is not None and c in FP64_STEPS_CAP) else None
+                snap = rec["fp64"]["steps"] if (q64 is not None and capped) else None
                 q32, r32 = run(q0, p, hc.FP32, fp32_stop, hc.HC_WARM_UNET if unet else hc.HC_WARM_PREVIOUS, wf,
                                max_steps=a.max_steps, log=log, snap=snap)
                 rho_snap = r32.pop("_snap", None)
@@ -218,12 +232,11 @@ def main():
                     r32.update(polytrope_figures(q0, q32, p))
                 rec[tag] = r32
                 del q32
+                save(out + [rec])
         print(json.dumps(rec), flush=True)
         out.append(rec)
         del q64
-        if a.out:   # written after every configuration
-            with open(a.out, "w") as f:
-                json.dump(out, f, indent=1)
+        save(out)
 
 
 if __name__ == "__main__":

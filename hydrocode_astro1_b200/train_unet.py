@@ -39,10 +39,12 @@ def make(problem, n, seed):
     raise SystemExit(f"unknown problem {problem}")
 
 
-def solver(q, p, warm=hc.HC_WARM_PREVIOUS):
+def solver(q, p, warm=hc.HC_WARM_PREVIOUS, weights=None):
     s = hc.HydroSolver3D(p["shape"], lo=p["lo"], hi=p["hi"], gamma=p["gamma"], G=p["G"], bc=p["bc"],
                          lmax=p["lmax"], cfl=p["cfl"], tol=1e-8, max_iter=2_000_000, precision=hc.FP32,
                          moment_order=hc.MOMENTS_TREE, warm_start=warm)
+    if weights:
+        s.unet_load_file(weights)
     s.set_state(q)
     return s
 
@@ -56,13 +58,26 @@ def _list(v, n, cast):
     return parts
 
 
-def collect(problem, n, seed, solves, every, skip, cycles, init_seed):
-    """A plain-solver run of the problem that records `solves` samples per
-    recorded cycle, one every `every` solves after `skip` unrecorded ones."""
+def collect(problem, n, seed, solves, every, skip, cycles, init_seed, with_weights=None):
+    """A run of the problem that records `solves` samples per recorded cycle,
+    one every `every` solves after `skip` unrecorded ones.  The run uses the
+    plain solver, or (with_weights) the learned start with those weights,
+    which reaches late steps sooner; a sample is the same either way: the
+    normalised first residual from the previous potential and the converged
+    correction of that potential."""
     q, p = make(problem, n, seed)
-    s = solver(q, p)
-    s.unet_collect(solves * len(cycles) + 1)
-    s.unet_init(init_seed)
+    if with_weights:
+        s = solver(q, p, hc.HC_WARM_UNET, with_weights)
+        params = s.unet_params()
+        s.unet_collect(solves * len(cycles) + 1)
+        s.unet_init(init_seed)              # training starts from a fresh network ...
+        fresh = s.unet_params()
+        s.unet_load(params[0], params[1])   # ... the run uses the given one
+    else:
+        s = solver(q, p)
+        s.unet_collect(solves * len(cycles) + 1)
+        s.unet_init(init_seed)
+        fresh = None
     iters = []
     for _ in range(skip):
         s.unet_record_cycle(0)
@@ -74,6 +89,8 @@ def collect(problem, n, seed, solves, every, skip, cycles, init_seed):
                 s.unet_record_cycle(c if k == every - 1 else 0)
                 s.step(1)
                 iters.append(s.diagnostics()["last_iterations"])
+    if fresh is not None:
+        s.unet_load(fresh[0], fresh[1])
     return s, iters
 
 
@@ -93,6 +110,8 @@ def main():
                     help="record every k-th solve (k - 1 unrecorded steps between samples), so that "
                          "`solves` samples span solves x k steps of the run (one, or per problem)")
     ap.add_argument("--skip", default="0", help="unrecorded steps before the first sample (one, or per problem)")
+    ap.add_argument("--collect-with", default=None, metavar="WEIGHTS",
+                    help="run the collection with the learned start from this weight file (faster late in a run)")
     ap.add_argument("--out", required=True)
     a = ap.parse_args()
     t0 = time.time()
@@ -101,7 +120,8 @@ def main():
     ns, seeds = _list(a.n, m, int), _list(a.seed, m, int)
     solves, every, skip = _list(a.solves, m, int), _list(a.record_every, m, int), _list(a.skip, m, int)
     cycles = [int(c) for c in a.record_cycles.split(",")]
-    runs = [collect(probs[q], ns[q], seeds[q], solves[q], every[q], skip[q], cycles, a.init_seed) for q in range(m)]
+    runs = [collect(probs[q], ns[q], seeds[q], solves[q], every[q], skip[q], cycles, a.init_seed, a.collect_with)
+            for q in range(m)]
     t_collect = time.time() - t0
     losses = []
     nchunk = 10 * m
@@ -128,7 +148,7 @@ def main():
     last.unet_save_file(a.out)
     tm = last.timing()
     report = {"problem": probs, "n": ns, "seed": seeds, "solves": solves, "record_cycles": cycles,
-              "record_every": every, "skip": skip,
+              "record_every": every, "skip": skip, "collected_with": a.collect_with,
               "samples": [r[0].unet_samples() for r in runs],
               "sor_iterations": [r[1] for r in runs], "train_steps": a.train_steps, "lr": a.lr,
               "init_seed": a.init_seed,
