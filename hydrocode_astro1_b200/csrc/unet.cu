@@ -327,11 +327,17 @@ cudaError_t conv_wgrad(UNetState *u, int l, const __nv_bfloat16 *x, const __nv_b
     return cudaGetLastError();
 }
 
-cudaError_t forward(UNetState *u, cudaStream_t s)
+// Forward pass from the single-channel input in u->pooled, scaled by 1 / rms
+// (sumsq != NULL: its sum of squares) or taken as is (sumsq == NULL).
+cudaError_t forward(UNetState *u, const double *sumsq, cudaStream_t s)
 {
     const Dims *L = u->L;
     cudaError_t e;
-    if ((e = conv_fwd(u, 0, u->x0, u->e[0], 0, 0, s))) return e;
+    // one thread per DK voxels along k; 128-thread blocks for the first (136
+    // registers: 64 packed accumulators), 256 for the last
+    const unsigned nfirst = (unsigned)std::min<long long>((L[0].n / DK + 127) / 128, 148LL * 12);
+    const unsigned ncol = (unsigned)std::min<long long>((L[0].n / DK + 255) / 256, 148LL * 8);
+    conv_first_kernel<<<nfirst, 128, 0, s>>>(u->pooled, sumsq, L[0], wf_of(u, 0), bias_of(u, 0), u->e[0]);
     for (int l = 1; l <= NLEV; l++) {
         pool2_kernel<<<nblk(L[l].n * 2), 256, 0, s>>>(u->e[l - 1], u->p[l], L[l]);
         if ((e = conv_fwd(u, l, u->p[l], u->e[l], l, 0, s))) return e;
@@ -342,7 +348,8 @@ cudaError_t forward(UNetState *u, cudaStream_t s)
         if ((e = conv_fwd(u, 2 * NLEV - l, u->sm[l], u->d[l], l, 0, s))) return e;
         h = u->d[l];
     }
-    return conv_fwd(u, NCONV - 1, u->d[0], u->out0, 0, 2, s);
+    conv_last_kernel<<<ncol, 256, 0, s>>>(u->d[0], L[0], wf_of(u, NCONV - 1), bias_of(u, NCONV - 1), u->out0);
+    return cudaGetLastError();
 }
 
 // gradients of the loss whose output gradient is in ga[0] (channel 0)
@@ -517,7 +524,9 @@ int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e
     const bool collect = record && u->cap > 0 && u->sx;
     u->slot = collect ? u->next : -1;
     float *xs = collect ? u->sx + (size_t)u->slot * u->L[0].n : nullptr;
-    in_norm_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->pooled, u->scal, u->L[0].n, u->x0, xs);
+    // the normalised input as a training sample (the prediction reads the
+    // pooled residual and its scale directly)
+    if (collect) in_norm_kernel<<<nblk(u->L[0].n * 2), 256, 0, s>>>(u->pooled, u->scal, u->L[0].n, u->x0, xs);
     if (collect) {
         if (u->phi0_n != a.g.n) {
             cudaFree(u->phi0);
@@ -528,7 +537,7 @@ int unet_begin_solve(UNetState *u, const GravArgs &a, const float *r32, float *e
     }
     if (e_out) {
         if (!u->have_weights) return HC_ERR_STATE;
-        if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+        if (forward(u, u->scal, s) != cudaSuccess) return HC_ERR_CUDA;
         out_up_kernel<<<(unsigned)(((long long)a.g.nx * a.g.ny + OUT_UP_ROWS - 1) / OUT_UP_ROWS), 128, 0, s>>>(
             u->out0, u->L[0], u->scal, u->kscale, sp, e_out);
     }
@@ -580,7 +589,7 @@ int unet_train(UNetState *u, int steps, double lr, unsigned seed, double *mean_l
         symmetry_kernel<<<nblk(n0), 256, 0, s>>>(u->sx + (size_t)smp * n0, u->pooled, d0, sym);
         symmetry_kernel<<<nblk(n0), 256, 0, s>>>(u->st + (size_t)smp * n0, u->xnorm, d0, sym);
         in_expand_kernel<<<nblk(n0 * 2), 256, 0, s>>>(u->pooled, n0, u->x0);
-        if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+        if (forward(u, nullptr, s) != cudaSuccess) return HC_ERR_CUDA;
         if (k == steps - tail) cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
         if (loss_grad(u, u->xnorm, u->st2[smp], s) != cudaSuccess) return HC_ERR_CUDA;
         if (backward(u, s) != cudaSuccess) return HC_ERR_CUDA;
@@ -612,7 +621,7 @@ int unet_loss_grad(UNetState *u, int n0x, int n0y, int n0z, const float *x, cons
     double t2 = 0.0;
     for (long long v = 0; v < n0; v++) t2 += (double)t[v] * t[v];
     in_expand_kernel<<<nblk(n0 * 2), 256, 0, s>>>(dx, n0, u->x0);
-    if (forward(u, s) != cudaSuccess) return HC_ERR_CUDA;
+    if (forward(u, nullptr, s) != cudaSuccess) return HC_ERR_CUDA;
     cudaMemsetAsync(u->scal + 2, 0, sizeof(double), s);
     cudaMemsetAsync(u->pg, 0, (size_t)NFULL * 4, s);
     if (loss_grad(u, dt, t2, s) != cudaSuccess) return HC_ERR_CUDA;
