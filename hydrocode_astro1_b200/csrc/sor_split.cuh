@@ -24,7 +24,6 @@
 // instead of sweeping; every later sweep of the batch then returns at once.
 #pragma once
 #include <cstdint>
-#include <cstdlib>
 #include <type_traits>
 #include "hc_internal.cuh"
 #include "hc_math.cuh"
@@ -244,58 +243,10 @@ struct alignas(16) Pack {
 // back unchanged.  Sweeps of colour 1 visit the planes in descending order
 // (each sweep starts where the previous one ended, where the L2 still holds
 // the shared colour arrays); the order does not change any result.
-// L2 prefetch of the rows a later CTA of the same sweep will load: the CTA
-// `ahead` places after this one in launch order (about one wave), its own
-// and source rows (NI planes x SPLIT_BY rows) and the other colour's rows
-// with their one-plane and one-row halo, one bulk prefetch per row segment
-// (16-byte aligned, a multiple of 16 bytes: H % V == 0), issued by the first
-// threads of the CTA.  Rows outside the grid are skipped.
-template <typename T, int NI>
-__device__ __forceinline__ void prefetch_ahead(const T *own, const T *oth, const T *src, const Split &sp, int colour,
-                                               int ahead)
-{
-    constexpr int V = Pack<T>::V;
-    const long long lin = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-    const long long tgt = lin + ahead;
-    const long long total = (long long)gridDim.x * gridDim.y * gridDim.z;
-    if (ahead <= 0 || tgt >= total) return;
-    const int tx = (int)(tgt % gridDim.x), ty = (int)((tgt / gridDim.x) % gridDim.y);
-    const int tz = (int)(tgt / ((long long)gridDim.x * gridDim.y));
-#if HC_SPLIT_SNAKE
-    const int bz = colour ? (int)gridDim.z - 1 - tz : tz;
-#else
-    const int bz = tz;
-#endif
-    const int i0 = 1 + bz * NI, j0 = ty * SPLIT_BY, m0 = tx * SPLIT_BX * V;
-    const int seg = min(SPLIT_BX * V, sp.H - m0);
-    if (seg <= 0) return;
-    const unsigned bytes = (unsigned)seg * (unsigned)sizeof(T);
-    // own and source: NI x SPLIT_BY rows each; other colour: (NI + 2) x (SPLIT_BY + 2)
-    constexpr int NO = NI * SPLIT_BY, NOT = (NI + 2) * (SPLIT_BY + 2);
-    const int t = threadIdx.y * SPLIT_BX + threadIdx.x;
-    if (t >= 2 * NO + NOT) return;
-    const T *base;
-    int i, j;
-    if (t < 2 * NO) {
-        const int q = t % NO;
-        base = t < NO ? own : src;
-        i = i0 + q / SPLIT_BY;
-        j = j0 + q % SPLIT_BY;
-    } else {
-        const int q = t - 2 * NO;
-        base = oth;
-        i = i0 - 1 + q / (SPLIT_BY + 2);
-        j = j0 - 1 + q % (SPLIT_BY + 2);
-    }
-    if (i < 0 || i >= sp.nx || j < 0 || j >= sp.ny) return;
-    const T *row = base + ((long long)i * sp.ny + j) * sp.H + m0;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"(bytes) : "memory");
-}
-
 template <typename T, int NI, int MINB>
 __global__ void __launch_bounds__(SPLIT_BX * SPLIT_BY, MINB)
 sor_split_vec_kernel(T *__restrict__ own, const T *__restrict__ oth, const T *__restrict__ src, Split sp,
-                     SorCoef<T> cf, int colour, double *res, int iter, double thresh, DevScalars *sc, int ahead)
+                     SorCoef<T> cf, int colour, double *res, int iter, double thresh, DevScalars *sc)
 {
     constexpr int V = Pack<T>::V;
     using P = Pack<T>;
@@ -312,7 +263,6 @@ sor_split_vec_kernel(T *__restrict__ own, const T *__restrict__ oth, const T *__
             return;
         }
     }
-    prefetch_ahead<T, NI>(own, oth, src, sp, colour, ahead);
     const int lane = threadIdx.x;
     const int m0 = (blockIdx.x * SPLIT_BX + lane) * V;
     const int j = blockIdx.y * SPLIT_BY + threadIdx.y;
@@ -426,23 +376,6 @@ __global__ void split_boundary_kernel(const T *__restrict__ nat, T *__restrict__
     }
 }
 
-// CTAs ahead of the current one whose rows a vector sweep prefetches into L2:
-// HC_SOR_PF waves (default 0: off) of `per_sm` CTAs on every SM.
-inline int sor_prefetch_ahead(int per_sm)
-{
-    static int waves = -1;
-    static int sms = 0;
-    if (waves < 0) {
-        const char *e = getenv("HC_SOR_PF");
-        waves = e ? atoi(e) : 0;
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
-                                                      cudaSuccess)
-            sms = 148;
-    }
-    return waves > 0 ? waves * per_sm * sms : 0;
-}
-
 template <typename T, typename S>
 cudaError_t launch_sor_split(T *base, const S *src, const Split &sp, const SorCoef<T> &cf, int colour,
                              double *res, int iter, double thresh, DevScalars *sc, cudaStream_t s)
@@ -460,7 +393,7 @@ cudaError_t launch_sor_split(T *base, const S *src, const Split &sp, const SorCo
         dim3 grid((sp.H / V + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + VNI - 1) / VNI);
         return launch_pdl(sor_split_vec_kernel<T, VNI, VMINB>, grid, dim3(SPLIT_BX, SPLIT_BY), s, own, oth,
                           reinterpret_cast<const T *>(src) + (size_t)colour * sp.cs, sp, cf, colour, res, iter, thresh,
-                          sc, sor_prefetch_ahead(VMINB));
+                          sc);
     }
 #endif
     dim3 grid((sp.H + SPLIT_BX - 1) / SPLIT_BX, (sp.ny + SPLIT_BY - 1) / SPLIT_BY, (sp.nx - 2 + NI - 1) / NI);
