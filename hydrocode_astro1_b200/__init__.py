@@ -99,6 +99,16 @@ CAPI = {
     "hc_get_signal_speed": (C.c_int, [C.c_void_p, _dp]),
     "hc_set_signal_speed": (C.c_int, [C.c_void_p, C.c_double]),
     "hc_copy_planes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
+    "hc_set_slab": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "hc_slab_moment_layout": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hc_slab_moments": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "hc_slab_set_moments": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int]),
+    "hc_slab_sor_begin": (C.c_int, [C.c_void_p]),
+    "hc_slab_sor_sweep": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "hc_slab_sor_boundary": (C.c_int, [C.c_void_p]),
+    "hc_slab_sor_norm": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "hc_slab_sor_end": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int]),
+    "hc_slab_phi_planes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "hc_set_conservation_record": (C.c_int, [C.c_void_p, C.c_int]),
     "hc_get_diag": (C.c_int, [C.c_void_p, C.POINTER(Diag)]),
     "hc_get_timing": (C.c_int, [C.c_void_p, C.POINTER(Timing), C.c_int]),
@@ -333,6 +343,53 @@ class HydroSolver3D:
         from (True) the device buffer at dev_ptr, field by field."""
         _check(self.L.hc_copy_planes(self.h, int(i0), int(count), C.c_void_p(int(dev_ptr)), int(bool(to_ctx))),
                "hc_copy_planes")
+
+    def set_slab(self, gnx, ioff):
+        """Declare this context the global planes [ioff, ioff + nx) of a grid
+        of gnx planes (its config's x bounds the whole grid's)."""
+        _check(self.L.hc_set_slab(self.h, int(gnx), int(ioff)), "hc_set_slab")
+
+    def slab_moment_layout(self, p):
+        """(sequential, width) of moment pass p across slabs."""
+        sq, w = C.c_int(0), C.c_int(0)
+        _check(self.L.hc_slab_moment_layout(self.h, int(p), C.byref(sq), C.byref(w)), "hc_slab_moment_layout")
+        return bool(sq.value), w.value
+
+    def slab_moments(self, p, buf):
+        """Pass p over the own planes: continues the sums in buf (sequential)
+        or fills buf with the own planes' partials; buf is FP64 numpy."""
+        assert buf.dtype == np.float64 and buf.flags.c_contiguous
+        _check(self.L.hc_slab_moments(self.h, int(p), buf.ctypes.data_as(_dp)), "hc_slab_moments")
+        return buf
+
+    def slab_set_moments(self, p, all_parts, nplanes):
+        a = np.ascontiguousarray(all_parts, dtype=np.float64)
+        _check(self.L.hc_slab_set_moments(self.h, int(p), a.ctypes.data_as(_dp), int(nplanes)),
+               "hc_slab_set_moments")
+
+    def slab_sor_begin(self):
+        _check(self.L.hc_slab_sor_begin(self.h), "hc_slab_sor_begin")
+
+    def slab_sor_sweep(self, it, colour):
+        _check(self.L.hc_slab_sor_sweep(self.h, int(it), int(colour)), "hc_slab_sor_sweep")
+
+    def slab_sor_boundary(self):
+        _check(self.L.hc_slab_sor_boundary(self.h), "hc_slab_sor_boundary")
+
+    def slab_sor_norm(self, it):
+        v = C.c_double(0.0)
+        _check(self.L.hc_slab_sor_norm(self.h, int(it), C.byref(v)), "hc_slab_sor_norm")
+        return v.value
+
+    def slab_sor_end(self, iterations, residual, converged):
+        _check(self.L.hc_slab_sor_end(self.h, int(iterations), float(residual), int(bool(converged))),
+               "hc_slab_sor_end")
+
+    def slab_phi_planes(self, i0, count, ptr, to_ctx):
+        """Planes [i0, i0+count) of the colour-split potential (both colours,
+        [2][count][ny (nz+1)/2] FP64) to (to_ctx False) or from (True) ptr."""
+        _check(self.L.hc_slab_phi_planes(self.h, int(i0), int(count), C.c_void_p(int(ptr)), int(bool(to_ctx))),
+               "hc_slab_phi_planes")
 
     def set_conservation_record(self, on=True):
         """Form the sums after every hc_step call (hc_diag 'cons')."""

@@ -120,6 +120,11 @@ struct hc_ctx {
     UnetGuard guard;             // learned-start outcome monitor (hc_set_unet_guard)
     double *cons_part;           // conservation sums: 5 * CONS_BLOCKS block partials
     int cons_record;             // 1: sums after every step, reported in hc_diag.cons
+    // a slab of a grid split along x (hc_set_slab): the Poisson solve runs
+    // across the slabs through the hc_slab_* entry points, not in hc_step
+    int slab;
+    double *slab_buf;            // moment sums / per-plane partials of the slab protocol
+    long long slab_buf_len;
     // checkpoints: device packing buffer, copy stream, writer thread
     unsigned char *ck_dev;
     size_t ck_dev_bytes;
@@ -219,7 +224,7 @@ static void free_ctx(hc_ctx *c)
             if (c->q32[b][v] && v == 0) cudaFree(c->q32[b][0]);
         }
     cudaFree(c->phi); cudaFree(c->phig); cudaFree(c->rho_ext); cudaFree(c->phi2);
-    cudaFree(c->phs); cudaFree(c->rhs); cudaFree(c->plm);
+    cudaFree(c->phs); cudaFree(c->rhs); cudaFree(c->plm); cudaFree(c->slab_buf);
     cudaFree(c->e32); cudaFree(c->r32); cudaFree(c->e32b);
     cudaFree(c->gx); cudaFree(c->gy); cudaFree(c->gz);
     cudaFree(c->res); cudaFree(c->scratch); cudaFree(c->mom); cudaFree(c->cons_part);
@@ -329,6 +334,7 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
     g.dx = k.dx > 0.0 ? k.dx : (k.xmax - k.xmin) / k.nx;
     g.dy = k.dy > 0.0 ? k.dy : (k.ymax - k.ymin) / k.ny;
     g.dz = k.dz > 0.0 ? k.dz : (k.zmax - k.zmin) / k.nz;
+    g.ioff = 0; g.gnx = k.nx; g.olo = 0; g.ohi = k.nx;
     c->gravity = k.G > 0.0;
     const size_t n = (size_t)g.n;
     int rc = HC_OK;
@@ -355,7 +361,7 @@ extern "C" hc_ctx *hc_create(const hc_config *cfg)
         if (!rc) rc = ensure_res(c, k.max_iter);
         // tree partials (592x9), lmax partials (<= 387x169), then the lmax
         // z-power sums (13 per (i, j) row)
-        c->scratch_len = 64 * 1024 + (long long)c->g.nx * c->g.ny * 13;
+        c->scratch_len = grav_scratch_len(c->g);
         if (!rc) rc = dmalloc((void **)&c->scratch, c->scratch_len * sizeof(double));
         if (!rc) rc = dmalloc((void **)&c->mom, 4 * 1024 * sizeof(double));
         if (!rc && k.precision == HC_FP32) {
@@ -972,6 +978,7 @@ extern "C" int hc_gravity_solve(hc_ctx *c, const double *rho, int with_accel)
 {
     if (!c) return set_err(HC_ERR_ARG, "null context");
     if (!c->gravity) return set_err(HC_ERR_STATE, "gravity disabled (G <= 0)");
+    if (c->slab) return set_err(HC_ERR_STATE, "a slab solves through the hc_slab_* entry points");
     CK(cudaSetDevice(c->dev));
     const size_t n = (size_t)c->g.n;
     int st;
@@ -1157,7 +1164,9 @@ static int step_once(hc_ctx *c, int *grav_status)
         c->cfl_valid = 1;
     }
     *grav_status = 1;
-    if (c->gravity) {
+    if (c->gravity && c->slab) {
+        *grav_status = c->diag.last_status;   // the solve ran across the slabs
+    } else if (c->gravity) {
         int st = f64 ? gravity_solve_dev(c, c->q64[c->cur][0], nullptr)
                      : gravity_solve_dev(c, nullptr, c->q32[c->cur][0]);
         if (st < -1) return st;
@@ -1442,6 +1451,228 @@ extern "C" int hc_copy_planes(hc_ctx *c, int i0, int count, void *buf, int to_ct
         char *f = field + (size_t)i0 * plane * word;
         char *b = static_cast<char *>(buf) + (size_t)v * bytes;
         CK(cudaMemcpyAsync(to_ctx ? f : b, to_ctx ? b : f, bytes, cudaMemcpyDefault, c->s));
+    }
+    return sync_ctx(c);
+}
+
+// ---------------------------------------------------------------- slabs: gravity
+// The Poisson solve of a grid split along x into slabs (FP64, isolated
+// boundary), driven across the slabs by the caller: the moment sums of the
+// own planes (chained in plane order, or per-plane partials gathered in
+// plane order), the red-black half sweeps with the ghost planes exchanged
+// after each, and the maximum of the slabs' update norms as the stop test
+// (gravity_solver_3d.c:510-747 on the whole grid).
+extern "C" int hc_set_slab(hc_ctx *c, int gnx, int ioff)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    const int nx = c->g.nx;
+    if (ioff < 0 || gnx < nx || ioff + nx > gnx)
+        return set_err(HC_ERR_ARG, "planes [%d, %d) outside a grid of %d", ioff, ioff + nx, gnx);
+    const int olo = ioff > 0 ? 1 : 0, ohi = ioff + nx < gnx ? nx - 1 : nx;
+    if (ohi - olo < 1) return set_err(HC_ERR_ARG, "a slab needs an own plane");
+    if (c->gravity) {
+        if (c->cfg.precision != HC_FP64) return set_err(HC_ERR_STATE, "slab gravity: FP64 contexts");
+        if (c->cfg.grav_bc != 1) return set_err(HC_ERR_STATE, "slab gravity: isolated boundary only");
+        if (c->g.nz < 3 || c->g.ny < 3) return set_err(HC_ERR_STATE, "slab gravity: ny, nz >= 3");
+        if (c->cfg.lmax == 0 && c->cfg.moment_order != HC_MOMENTS_SEQUENTIAL &&
+            c->cfg.moment_order != HC_MOMENTS_TREE)
+            return set_err(HC_ERR_STATE, "slab gravity: sequential or tree moments");
+    }
+    Geom &g = c->g;
+    g.ioff = ioff;
+    g.gnx = gnx;
+    g.olo = olo;
+    g.ohi = ohi;
+    if (!(c->cfg.dx > 0.0)) g.dx = (c->cfg.xmax - c->cfg.xmin) / gnx;
+    c->slab = 1;
+    return HC_OK;
+}
+
+static bool slab_sequential(const hc_ctx *c)
+{
+    return c->cfg.lmax == 0 && c->cfg.moment_order == HC_MOMENTS_SEQUENTIAL;
+}
+
+// Doubles per own plane of a pass's partials (or, sequential, the sums).
+static int slab_width(const hc_ctx *c, int pass)
+{
+    if (c->cfg.lmax == 0) return pass == 0 ? 4 : 9;
+    return pass == 0 ? 4 : lmax_slab_width(c->g);
+}
+
+static int slab_ready(hc_ctx *c)
+{
+    if (!c) return set_err(HC_ERR_ARG, "null context");
+    if (!c->slab || !c->gravity) return set_err(HC_ERR_STATE, "not a self-gravitating slab (hc_set_slab)");
+    if (c->cfg.gravity_only) return set_err(HC_ERR_STATE, "gravity-only context");
+    CK(cudaSetDevice(c->dev));
+    return HC_OK;
+}
+
+static int slab_buffer(hc_ctx *c, long long need)
+{
+    if (c->slab_buf && c->slab_buf_len >= need) return HC_OK;
+    cudaFree(c->slab_buf);
+    c->slab_buf = nullptr;
+    int rc = dmalloc((void **)&c->slab_buf, (size_t)need * sizeof(double));
+    if (rc) return rc;
+    c->slab_buf_len = need;
+    return HC_OK;
+}
+
+extern "C" int hc_slab_moment_layout(hc_ctx *c, int pass, int *sequential, int *width)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if ((pass != 0 && pass != 1) || !sequential || !width) return set_err(HC_ERR_ARG, "bad argument");
+    *sequential = slab_sequential(c) ? 1 : 0;
+    *width = slab_width(c, pass);
+    return HC_OK;
+}
+
+extern "C" int hc_slab_moments(hc_ctx *c, int pass, double *buf)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if ((pass != 0 && pass != 1) || !buf) return set_err(HC_ERR_ARG, "bad argument");
+    GravArgs a = grav_args(c, c->q64[c->cur][0], nullptr);
+    const int w = slab_width(c, pass);
+    const int np = c->g.ohi - c->g.olo;
+    const long long count = slab_sequential(c) ? w : (long long)np * w;
+    rc = slab_buffer(c, count);
+    if (rc) return rc;
+    {
+        FamTimer t(c, FAM_MOM);
+        if (slab_sequential(c)) {
+            CK(cudaMemcpyAsync(c->slab_buf, buf, count * sizeof(double), cudaMemcpyHostToDevice, c->s));
+            CK(grav_moments_seq_slab(a, pass, c->slab_buf, c->s));
+        } else if (c->cfg.lmax == 0) {
+            CK(grav_moments_tree_parts(a, pass, c->slab_buf, c->s));
+        } else {
+            CK(grav_moments_lmax_parts(a, pass, c->slab_buf, c->s));
+        }
+        c->launches += 1;
+    }
+    CK(cudaMemcpyAsync(buf, c->slab_buf, count * sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    return sync_ctx(c);
+}
+
+extern "C" int hc_slab_set_moments(hc_ctx *c, int pass, const double *all, int nplanes)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if ((pass != 0 && pass != 1) || !all) return set_err(HC_ERR_ARG, "bad argument");
+    const int w = slab_width(c, pass);
+    if (!slab_sequential(c) && nplanes != c->g.gnx)
+        return set_err(HC_ERR_ARG, "partials of %d planes for a grid of %d", nplanes, c->g.gnx);
+    const long long count = slab_sequential(c) ? w : (long long)nplanes * w;
+    rc = slab_buffer(c, count);
+    if (rc) return rc;
+    GravArgs a = grav_args(c, c->q64[c->cur][0], nullptr);
+    FamTimer t(c, FAM_MOM);
+    CK(cudaMemcpyAsync(c->slab_buf, all, count * sizeof(double), cudaMemcpyHostToDevice, c->s));
+    if (slab_sequential(c)) CK(grav_moments_seq_set(a, pass, c->slab_buf, c->s));
+    else if (c->cfg.lmax == 0) CK(grav_moments_tree_set(a, pass, c->slab_buf, nplanes, c->s));
+    else CK(grav_moments_lmax_set(a, pass, c->slab_buf, nplanes, c->s));
+    c->launches += 1;
+    return sync_ctx(c);
+}
+
+extern "C" int hc_slab_sor_begin(hc_ctx *c)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    GravArgs a = grav_args(c, c->q64[c->cur][0], nullptr);
+    rc = ensure_res(c, a.max_iter);
+    if (rc) return rc;
+    a.res = c->res;
+    const size_t ns = (size_t)split_len(c->g);
+    if (!c->phs) rc = dmalloc((void **)&c->phs, ns * sizeof(double));
+    if (!rc && !c->rhs) rc = dmalloc((void **)&c->rhs, ns * sizeof(double));
+    if (rc) return rc;
+    if (!c->hslots && cudaMallocHost((void **)&c->hslots, 512 * sizeof(double)) != cudaSuccess)
+        return set_err(HC_ERR_NOMEM, "pinned slot buffer");
+    CK(cudaMemsetAsync(&c->sc->done, 0, 2 * sizeof(int), c->s));
+    CK(grav_reset_slots(a, 0, std::max(a.max_iter, 1), c->s));
+    CK(grav_split_fields(a, c->phs, c->rhs, c->s));
+    c->launches += 3;
+    return HC_OK;
+}
+
+// One half sweep of the whole grid's colour (local colour colour ^ ioff).
+extern "C" int hc_slab_sor_sweep(hc_ctx *c, int iter, int colour)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if (iter < 0 || iter >= c->cfg.max_iter || (colour != 0 && colour != 1) || !c->phs)
+        return set_err(HC_ERR_ARG, "bad sweep (iteration %d, colour %d)", iter, colour);
+    GravArgs a = grav_args(c, c->q64[c->cur][0], nullptr);
+    a.res = c->res;
+    a.tol = -1.0;   // the stop test is the caller's, over all slabs
+    FamTimer t(c, FAM_SOR);
+    CK(grav_sor_split(a, c->phs, c->rhs, colour ^ (c->g.ioff & 1), iter, c->s));
+    c->launches += 1;
+    c->sor_launches += 1;
+    return HC_OK;
+}
+
+extern "C" int hc_slab_sor_boundary(hc_ctx *c)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if (!c->phs) return set_err(HC_ERR_STATE, "hc_slab_sor_begin first");
+    GravArgs a = grav_args(c, c->q64[c->cur][0], nullptr);
+    rc = grav_boundary_values(c, a);
+    if (rc) return rc;
+    CK(grav_split_boundary(a, c->phs, c->s));
+    c->launches += 1;
+    return HC_OK;
+}
+
+extern "C" int hc_slab_sor_norm(hc_ctx *c, int iter, double *norm)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if (iter < 0 || iter >= c->cfg.max_iter || !norm) return set_err(HC_ERR_ARG, "bad argument");
+    if (!c->hslots) return set_err(HC_ERR_STATE, "hc_slab_sor_begin first");
+    CK(cudaMemcpyAsync(c->hslots, c->res + iter, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+    rc = sync_ctx(c);
+    if (rc) return rc;
+    *norm = c->hslots[0];
+    return HC_OK;
+}
+
+extern "C" int hc_slab_sor_end(hc_ctx *c, int iterations, double residual, int converged)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if (!c->phs) return set_err(HC_ERR_STATE, "hc_slab_sor_begin first");
+    GravArgs a = grav_args(c, c->q64[c->cur][0], nullptr);
+    CK(grav_unsplit(a, c->phs, c->s));
+    c->launches += 1;
+    c->diag.last_iterations = iterations;
+    c->diag.last_residual = residual;
+    c->diag.total_iterations += iterations;
+    c->diag.last_status = converged ? 0 : -1;
+    if (converged) CK(cudaMemcpyAsync(c->phig, c->phi, (size_t)c->g.n * sizeof(double), cudaMemcpyDeviceToDevice, c->s));
+    return sync_ctx(c);
+}
+
+// Planes [i0, i0 + count) of the colour-split potential, both colours:
+// buf holds [2][count][ny * ((nz + 1) / 2)] doubles.
+extern "C" int hc_slab_phi_planes(hc_ctx *c, int i0, int count, void *buf, int to_ctx)
+{
+    int rc = slab_ready(c);
+    if (rc) return rc;
+    if (!buf || !c->phs || i0 < 0 || count < 0 || i0 + count > c->g.nx || (to_ctx != 0 && to_ctx != 1))
+        return set_err(HC_ERR_ARG, "bad argument");
+    const size_t plane = (size_t)c->g.ny * ((c->g.nz + 1) / 2);
+    const size_t cs = (size_t)c->g.nx * plane, bytes = (size_t)count * plane * sizeof(double);
+    for (int q = 0; q < 2; q++) {
+        double *f = c->phs + q * cs + (size_t)i0 * plane;
+        char *b = static_cast<char *>(buf) + q * bytes;
+        CK(cudaMemcpyAsync(to_ctx ? (void *)f : (void *)b, to_ctx ? (const void *)b : (const void *)f, bytes,
+                           cudaMemcpyDefault, c->s));
     }
     return sync_ctx(c);
 }

@@ -51,130 +51,131 @@ constexpr int SEQ_NT = 256;
 
 // Bit-exact moments: terms per cell are formed in parallel into shared
 // memory, then one thread per accumulator adds them in cell order.
+
+// The terms of cell c: pass 0 (dm, dm x, dm y, dm z), pass 1 the quadrupole
+// terms about com (gravity_solver_3d.c:181-190, :236-255); zero where rho <= 0.
+__device__ __forceinline__ void seq_terms(const GravArgs &a, int pass, long long c, const double *com, double *t)
+{
+    const Geom &g = a.g;
+    const double r = a.rho ? a.rho[c] : (double)a.rho32[c];
+    if (!(r > 0.0)) return;
+    const long long snz = g.nz, sjk = (long long)g.ny * g.nz;
+    const int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
+    const double dm = r * (g.dx * g.dy * g.dz);
+    if (pass == 0) {
+        double x = g.xmin + (i + g.ioff + 0.5) * g.dx;
+        double y = g.ymin + (j + 0.5) * g.dy;
+        double z = g.zmin + (k + 0.5) * g.dz;
+        t[0] = dm; t[1] = dm * x; t[2] = dm * y; t[3] = dm * z;
+    } else {
+        double x = g.xmin + (i + g.ioff + 0.5) * g.dx - com[0];
+        double y = g.ymin + (j + 0.5) * g.dy - com[1];
+        double z = g.zmin + (k + 0.5) * g.dz - com[2];
+        double r2 = x * x + y * y + z * z;
+        t[0] = dm * (3.0 * x * x - r2);
+        t[1] = dm * (3.0 * x * y);
+        t[2] = dm * (3.0 * x * z);
+        t[3] = dm * (3.0 * y * x);
+        t[4] = dm * (3.0 * y * y - r2);
+        t[5] = dm * (3.0 * y * z);
+        t[6] = dm * (3.0 * z * x);
+        t[7] = dm * (3.0 * z * y);
+        t[8] = dm * (3.0 * z * z - r2);
+    }
+}
+
+// One pass over the cells [c0, c1) in order: thread q < nv returns acc plus
+// term q of every cell, added one by one.
+__device__ double seq_pass(const GravArgs &a, int pass, long long c0, long long c1, const double *com,
+                           double *term, double acc)
+{
+    const int tid = threadIdx.x;
+    const int nv = pass == 0 ? 4 : 9;
+    for (long long base = c0; base < c1; base += SEQ_CH) {
+        for (int e = tid; e < SEQ_CH; e += SEQ_NT) {
+            const long long c = base + e;
+            double t[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+            if (c < c1) seq_terms(a, pass, c, com, t);
+            for (int q = 0; q < nv; q++) term[q * SEQ_CH + e] = t[q];
+        }
+        __syncthreads();
+        if (tid < nv) {
+            const double *tt = term + tid * SEQ_CH;
+            const int m = (int)min((long long)SEQ_CH, c1 - base);
+            for (int e = 0; e < m; e++) acc += tt[e];
+        }
+        __syncthreads();
+    }
+    return acc;
+}
+
+__device__ __forceinline__ void centre_of_mass(const Geom &g, const double *acc, double *out)
+{
+    const double M = acc[0];
+    out[0] = M;
+    if (M > 0.0) {
+        out[1] = acc[1] / M; out[2] = acc[2] / M; out[3] = acc[3] / M;
+    } else {
+        out[1] = 0.5 * (g.xmin + g.xmax);
+        out[2] = 0.5 * (g.ymin + g.ymax);
+        out[3] = 0.5 * (g.zmin + g.zmax);
+    }
+}
+
 __global__ void __launch_bounds__(SEQ_NT) moments_seq_kernel(GravArgs a)
 {
     extern __shared__ double term[];   // 9 x SEQ_CH
     __shared__ double accs[9];
-    const Geom g = a.g;
+    __shared__ double mc[4];
     const int tid = threadIdx.x;
-    const double dV = g.dx * g.dy * g.dz;
-    const long long n = g.n, snz = g.nz, sjk = (long long)g.ny * g.nz;
-    double acc = 0.0;
-    // pass 1: M, sum dm*x, sum dm*y, sum dm*z
-    for (long long base = 0; base < n; base += SEQ_CH) {
-        for (int e = tid; e < SEQ_CH; e += SEQ_NT) {
-            long long c = base + e;
-            double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
-            if (c < n) {
-                double r = a.rho[c];
-                if (r > 0.0) {
-                    int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
-                    double x = g.xmin + (i + 0.5) * g.dx;
-                    double y = g.ymin + (j + 0.5) * g.dy;
-                    double z = g.zmin + (k + 0.5) * g.dz;
-                    double dm = r * dV;
-                    t0 = dm; t1 = dm * x; t2 = dm * y; t3 = dm * z;
-                }
-            }
-            term[0 * SEQ_CH + e] = t0; term[1 * SEQ_CH + e] = t1;
-            term[2 * SEQ_CH + e] = t2; term[3 * SEQ_CH + e] = t3;
-        }
-        __syncthreads();
-        if (tid < 4) {
-            const double *tt = term + tid * SEQ_CH;
-            int m = (int)min((long long)SEQ_CH, n - base);
-            for (int e = 0; e < m; e++) acc += tt[e];
-        }
-        __syncthreads();
-    }
+    const long long n = a.g.n;
+    double acc = seq_pass(a, 0, 0, n, nullptr, term, 0.0);
     if (tid < 4) accs[tid] = acc;
     __syncthreads();
-    double M = accs[0], xc, yc, zc;
-    if (M > 0.0) { xc = accs[1] / M; yc = accs[2] / M; zc = accs[3] / M; }
-    else {
-        xc = 0.5 * (g.xmin + g.xmax);
-        yc = 0.5 * (g.ymin + g.ymax);
-        zc = 0.5 * (g.zmin + g.zmax);
-    }
+    if (tid == 0) centre_of_mass(a.g, accs, mc);
     __syncthreads();
-    acc = 0.0;
-    // pass 2: Q_ij about the centre of mass
-    for (long long base = 0; base < n; base += SEQ_CH) {
-        for (int e = tid; e < SEQ_CH; e += SEQ_NT) {
-            long long c = base + e;
-            double t[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
-            if (c < n) {
-                double r = a.rho[c];
-                if (r > 0.0) {
-                    int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
-                    double x = g.xmin + (i + 0.5) * g.dx - xc;
-                    double y = g.ymin + (j + 0.5) * g.dy - yc;
-                    double z = g.zmin + (k + 0.5) * g.dz - zc;
-                    double dm = r * dV;
-                    double r2 = x * x + y * y + z * z;
-                    t[0] = dm * (3.0 * x * x - r2);
-                    t[1] = dm * (3.0 * x * y);
-                    t[2] = dm * (3.0 * x * z);
-                    t[3] = dm * (3.0 * y * x);
-                    t[4] = dm * (3.0 * y * y - r2);
-                    t[5] = dm * (3.0 * y * z);
-                    t[6] = dm * (3.0 * z * x);
-                    t[7] = dm * (3.0 * z * y);
-                    t[8] = dm * (3.0 * z * z - r2);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 9; q++) term[q * SEQ_CH + e] = t[q];
-        }
-        __syncthreads();
-        if (tid < 9) {
-            const double *tt = term + tid * SEQ_CH;
-            int m = (int)min((long long)SEQ_CH, n - base);
-            for (int e = 0; e < m; e++) acc += tt[e];
-        }
-        __syncthreads();
-    }
-    if (tid == 0) {
-        a.sc->moments[0] = M; a.sc->moments[1] = xc; a.sc->moments[2] = yc; a.sc->moments[3] = zc;
-    }
+    acc = seq_pass(a, 1, 0, n, mc + 1, term, 0.0);
+    if (tid < 4) a.sc->moments[tid] = mc[tid];
     if (tid < 9) a.sc->moments[4 + tid] = acc;
 }
 
-// Deterministic tree: fixed grid, per-block partials in a fixed order.
-constexpr int TREE_NT = 256;
-constexpr int TREE_NB = 592;
+// A slab's share of the sequential sums: the own planes, continuing acc.
+__global__ void __launch_bounds__(SEQ_NT) moments_seq_slab_kernel(GravArgs a, int pass, double *acc)
+{
+    extern __shared__ double term[];
+    const int tid = threadIdx.x;
+    const int nv = pass == 0 ? 4 : 9;
+    const long long sjk = (long long)a.g.ny * a.g.nz;
+    double v = tid < nv ? acc[tid] : 0.0;
+    v = seq_pass(a, pass, a.g.olo * sjk, a.g.ohi * sjk, a.sc->moments + 1, term, v);
+    if (tid < nv) acc[tid] = v;
+}
 
-__global__ void __launch_bounds__(TREE_NT) moments_tree_partial(GravArgs a, int pass)
+__global__ void moments_seq_set_kernel(GravArgs a, int pass, const double *acc)
+{
+    if (threadIdx.x != 0) return;
+    if (pass == 0) centre_of_mass(a.g, acc, a.sc->moments);
+    else
+        for (int t = 0; t < 9; t++) a.sc->moments[4 + t] = acc[t];
+}
+
+// Deterministic tree: one CTA per plane (thread-strided cells, warp and
+// block sums in a fixed order), then the planes' partials added in plane
+// order -- a fixed order that a grid split into slabs of planes reproduces.
+constexpr int TREE_NT = 256;
+
+__global__ void __launch_bounds__(TREE_NT) moments_tree_partial(GravArgs a, int pass, double *parts)
 {
     const Geom g = a.g;
-    const double dV = g.dx * g.dy * g.dz;
-    const long long n = g.n, snz = g.nz, sjk = (long long)g.ny * g.nz;
-    double xc = 0, yc = 0, zc = 0;
-    if (pass == 1) { xc = a.sc->moments[1]; yc = a.sc->moments[2]; zc = a.sc->moments[3]; }
+    const long long sjk = (long long)g.ny * g.nz;
+    const long long c0 = (long long)(g.olo + blockIdx.x) * sjk;
     const int nv = pass == 0 ? 4 : 9;
+    const double *com = a.sc->moments + 1;
     double acc[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
-    for (long long c = blockIdx.x * (long long)TREE_NT + threadIdx.x; c < n;
-         c += (long long)TREE_NB * TREE_NT) {
-        double r = a.rho ? a.rho[c] : (double)a.rho32[c];
-        if (!(r > 0.0)) continue;
-        int i = (int)(c / sjk), j = (int)((c / snz) % g.ny), k = (int)(c % snz);
-        double dm = r * dV;
-        if (pass == 0) {
-            double x = g.xmin + (i + 0.5) * g.dx;
-            double y = g.ymin + (j + 0.5) * g.dy;
-            double z = g.zmin + (k + 0.5) * g.dz;
-            acc[0] += dm; acc[1] += dm * x; acc[2] += dm * y; acc[3] += dm * z;
-        } else {
-            double x = g.xmin + (i + 0.5) * g.dx - xc;
-            double y = g.ymin + (j + 0.5) * g.dy - yc;
-            double z = g.zmin + (k + 0.5) * g.dz - zc;
-            double r2 = x * x + y * y + z * z;
-            acc[0] += dm * (3.0 * x * x - r2); acc[1] += dm * (3.0 * x * y);
-            acc[2] += dm * (3.0 * x * z);      acc[3] += dm * (3.0 * y * x);
-            acc[4] += dm * (3.0 * y * y - r2); acc[5] += dm * (3.0 * y * z);
-            acc[6] += dm * (3.0 * z * x);      acc[7] += dm * (3.0 * z * y);
-            acc[8] += dm * (3.0 * z * z - r2);
-        }
+    for (long long c = c0 + threadIdx.x; c < c0 + sjk; c += TREE_NT) {
+        double t[9] = { 0, 0, 0, 0, 0, 0, 0, 0, 0 };
+        seq_terms(a, pass, c, com, t);
+        for (int q = 0; q < nv; q++) acc[q] += t[q];
     }
     __shared__ double red[TREE_NT / 32][9];
     for (int q = 0; q < nv; q++) {
@@ -187,33 +188,24 @@ __global__ void __launch_bounds__(TREE_NT) moments_tree_partial(GravArgs a, int 
     if (threadIdx.x < nv) {
         double s = 0.0;
         for (int w = 0; w < TREE_NT / 32; w++) s += red[w][threadIdx.x];
-        a.scratch[(long long)blockIdx.x * 9 + threadIdx.x] = s;
+        parts[(long long)blockIdx.x * 9 + threadIdx.x] = s;
     }
 }
 
-__global__ void moments_tree_final(GravArgs a, int pass)
+__global__ void moments_tree_final(GravArgs a, int pass, const double *parts, int nparts)
 {
     const int q = threadIdx.x;
     const int nv = pass == 0 ? 4 : 9;
     __shared__ double v[9];
     if (q < nv) {
         double s = 0.0;
-        for (int b = 0; b < TREE_NB; b++) s += a.scratch[(long long)b * 9 + q];
+        for (int b = 0; b < nparts; b++) s += parts[(long long)b * 9 + q];
         v[q] = s;
     }
     __syncthreads();
     if (q != 0) return;
-    const Geom g = a.g;
     if (pass == 0) {
-        double M = v[0];
-        a.sc->moments[0] = M;
-        if (M > 0.0) {
-            a.sc->moments[1] = v[1] / M; a.sc->moments[2] = v[2] / M; a.sc->moments[3] = v[3] / M;
-        } else {
-            a.sc->moments[1] = 0.5 * (g.xmin + g.xmax);
-            a.sc->moments[2] = 0.5 * (g.ymin + g.ymax);
-            a.sc->moments[3] = 0.5 * (g.zmin + g.zmax);
-        }
+        centre_of_mass(a.g, v, a.sc->moments);
     } else {
         for (int t = 0; t < 9; t++) a.sc->moments[4 + t] = v[t];
     }
@@ -245,7 +237,7 @@ __device__ __forceinline__ double mono_quad(double x, double y, double z, const 
 __device__ __forceinline__ void face_point(const Geom &g, int i, int j, int k, bool zb,
                                            double &x, double &y, double &z)
 {
-    x = g.xmin + (i + 0.5) * g.dx;
+    x = g.xmin + (i + g.ioff + 0.5) * g.dx;
     y = g.ymin + (j + 0.5) * g.dy;
     z = g.zmin + (k + 0.5) * g.dz;
     if (zb && (k == 0 || k == g.nz - 1)) {
@@ -253,7 +245,7 @@ __device__ __forceinline__ void face_point(const Geom &g, int i, int j, int k, b
     } else if (j == 0 || j == g.ny - 1) {
         y = (j == g.ny - 1) ? g.ymax - 0.5 * g.dy : g.ymin + 0.5 * g.dy;
     } else {
-        x = (i == g.nx - 1) ? g.xmax - 0.5 * g.dx : g.xmin + 0.5 * g.dx;
+        x = (i + g.ioff == g.gnx - 1) ? g.xmax - 0.5 * g.dx : g.xmin + 0.5 * g.dx;
     }
 }
 
@@ -266,6 +258,7 @@ __global__ void boundary_ref_kernel(GravArgs a)
     if (t >= nb) return;
     int i, j, k;
     boundary_cell(t, g.nx, g.ny, g.nz, zb, i, j, k);
+    if (i < g.olo || i >= g.ohi) return;   // a ghost plane: the neighbour's cells
     double x, y, z;
     face_point(g, i, j, k, zb, x, y, z);
     a.phi[((long long)i * g.ny + j) * g.nz + k] = mono_quad(x, y, z, a.sc->moments, a.G);
@@ -438,14 +431,45 @@ cudaError_t grav_moments_sequential(const GravArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+cudaError_t grav_moments_seq_slab(const GravArgs &a, int pass, double *acc, cudaStream_t s)
+{
+    const size_t sm = 9 * SEQ_CH * sizeof(double);
+    static std::atomic<unsigned long long> attr_set{0};
+    cudaError_t e = set_smem_once(attr_set, (const void *)moments_seq_slab_kernel, (int)sm);
+    if (e != cudaSuccess) return e;
+    moments_seq_slab_kernel<<<1, SEQ_NT, sm, s>>>(a, pass, acc);
+    return cudaGetLastError();
+}
+
+cudaError_t grav_moments_seq_set(const GravArgs &a, int pass, const double *acc, cudaStream_t s)
+{
+    moments_seq_set_kernel<<<1, 32, 0, s>>>(a, pass, acc);
+    return cudaGetLastError();
+}
+
+cudaError_t grav_moments_tree_parts(const GravArgs &a, int pass, double *parts, cudaStream_t s)
+{
+    if (a.g.ohi <= a.g.olo) return cudaErrorInvalidValue;
+    moments_tree_partial<<<a.g.ohi - a.g.olo, TREE_NT, 0, s>>>(a, pass, parts);
+    return cudaGetLastError();
+}
+
+cudaError_t grav_moments_tree_set(const GravArgs &a, int pass, const double *parts, int nparts, cudaStream_t s)
+{
+    moments_tree_final<<<1, 32, 0, s>>>(a, pass, parts, nparts);
+    return cudaGetLastError();
+}
+
 cudaError_t grav_moments_tree(const GravArgs &a, cudaStream_t s)
 {
-    if (a.scratch_len < (long long)TREE_NB * 9) return cudaErrorInvalidValue;
+    if (a.scratch_len < (long long)a.g.nx * 9) return cudaErrorInvalidValue;
     for (int pass = 0; pass < 2; pass++) {
-        moments_tree_partial<<<TREE_NB, TREE_NT, 0, s>>>(a, pass);
-        moments_tree_final<<<1, 32, 0, s>>>(a, pass);
+        cudaError_t e = grav_moments_tree_parts(a, pass, a.scratch, s);
+        if (e != cudaSuccess) return e;
+        e = grav_moments_tree_set(a, pass, a.scratch, a.g.ohi - a.g.olo, s);
+        if (e != cudaSuccess) return e;
     }
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 cudaError_t grav_boundary_ref(const GravArgs &a, cudaStream_t s)

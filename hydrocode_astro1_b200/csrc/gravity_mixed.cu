@@ -32,7 +32,6 @@ namespace {
 
 constexpr int LM_MAX = 12;
 constexpr int LM_NC = (LM_MAX + 1) * (LM_MAX + 1);
-constexpr long long LM_SCRATCH0 = 64 * 1024;   // doubles of partial sums before the z-power sums
 
 __constant__ double c_norm[LM_NC];   // N_lm at l*(LM_MAX+1)+m
 
@@ -97,17 +96,17 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-// Centre of mass, partial sums per CTA: (S0, x S0, y S0, S1) over its rows,
-// S0 = sum_k rho, S1 = sum_k rho z (cells with rho > 0, as in every moment).
-__global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a)
+// Centre of mass, one partial per own plane (CTA): (S0, x S0, y S0, S1) over
+// its rows, S0 = sum_k rho, S1 = sum_k rho z (cells with rho > 0, as in
+// every moment); warp w takes rows w, w + 8, ...
+__global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a, double *parts)
 {
     const Geom g = a.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long rows = (long long)g.nx * g.ny;
+    const int i = g.olo + blockIdx.x;
     double v0 = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
-    for (long long row = (long long)blockIdx.x * (LR_NT / 32) + warp; row < rows;
-         row += (long long)gridDim.x * (LR_NT / 32)) {
-        const long long base = row * g.nz;
+    for (int j = warp; j < g.ny; j += LR_NT / 32) {
+        const long long base = ((long long)i * g.ny + j) * g.nz;
         double s0 = 0.0, s1 = 0.0;
         for (int k0 = 0; k0 < g.nz; k0 += 32 * LR_UNROLL) {
             double rv[LR_UNROLL];
@@ -126,9 +125,8 @@ __global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a)
         }
         s0 = warp_sum(s0);
         s1 = warp_sum(s1);
-        const int i = (int)(row / g.ny), j = (int)(row % g.ny);
         v0 += s0;
-        vx += (g.xmin + (i + 0.5) * g.dx) * s0;
+        vx += (g.xmin + (i + g.ioff + 0.5) * g.dx) * s0;
         vy += (g.ymin + (j + 0.5) * g.dy) * s0;
         vz += s1;
     }
@@ -143,19 +141,19 @@ __global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a)
     if (threadIdx.x < 4) {
         double s = 0.0;
         for (int w = 0; w < LR_NT / 32; w++) s += red[w][threadIdx.x];
-        a.scratch[(long long)blockIdx.x * 4 + threadIdx.x] = s;
+        parts[(long long)blockIdx.x * 4 + threadIdx.x] = s;
     }
 }
 
 // M = dV S0 and the centre of mass (box centre when there is no mass), as
 // the reference's monopole pass stores them.  Warp q adds the partials of
 // sum q (lane-strided, then a fixed butterfly).
-__global__ void __launch_bounds__(128) lmax_com_final(GravArgs a, int nparts)
+__global__ void __launch_bounds__(128) lmax_com_final(GravArgs a, const double *parts, int nparts)
 {
     __shared__ double v[4];
     const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double s = 0.0;
-    for (int b = lane; b < nparts; b += 32) s += a.scratch[(long long)b * 4 + q];
+    for (int b = lane; b < nparts; b += 32) s += parts[(long long)b * 4 + q];
     s = warp_sum(s);
     if (lane == 0) v[q] = s;
     __syncthreads();
@@ -180,8 +178,9 @@ __global__ void __launch_bounds__(LR_NT) lmax_zsums(GravArgs a, const double *co
     const Geom g = a.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long rows = (long long)g.nx * g.ny;
+    const long long row1 = (long long)g.ohi * g.ny;
     const double z0 = g.zmin - com[2];
-    for (long long row = (long long)blockIdx.x * (LR_NT / 32) + warp; row < rows;
+    for (long long row = (long long)g.olo * g.ny + (long long)blockIdx.x * (LR_NT / 32) + warp; row < row1;
          row += (long long)gridDim.x * (LR_NT / 32)) {
         const long long base = row * g.nz;
         double acc[LMAX + 1];
@@ -217,24 +216,28 @@ __global__ void __launch_bounds__(LR_NT) lmax_zsums(GravArgs a, const double *co
     }
 }
 
-// Order m = blockIdx.y; each thread takes rows blockIdx.x * LR_ROWBLK +
-// threadIdx.x, + gridDim.x * LR_ROWBLK, ...; the block's sums of
-// dV N_lm Q_m^m sum_t c_lt Z_t go to its partial slots (l*l+l+m for the real
-// part, l*l+l-m for the imaginary part), which lmax_final adds in block order.
+// Order m = blockIdx.y; block x covers rows q LR_ROWBLK .. of own plane
+// olo + x / QR (q = x % QR, QR = ceil(ny / LR_ROWBLK)), one row per thread;
+// the block's sums of dV N_lm Q_m^m sum_t c_lt Z_t go to its partial slots
+// (l*l+l+m for the real part, l*l+l-m for the imaginary part), which
+// lmax_final adds in block order.
 template <int LMAX>
-__global__ void __launch_bounds__(LR_ROWBLK) lmax_rows(GravArgs a, const double *com, const double *zs)
+__global__ void __launch_bounds__(LR_ROWBLK) lmax_rows(GravArgs a, const double *com, const double *zs,
+                                                       double *parts)
 {
     const Geom g = a.g;
     const int m = blockIdx.y;
     const long long rows = (long long)g.nx * g.ny;
+    const int QR = (g.ny + LR_ROWBLK - 1) / LR_ROWBLK;
+    const int i = g.olo + (int)blockIdx.x / QR;
+    const int j = ((int)blockIdx.x % QR) * LR_ROWBLK + threadIdx.x;
     const double xc = com[0], yc = com[1];
     double ar[LMAX + 1], ai[LMAX + 1];
 #pragma unroll
     for (int d = 0; d <= LMAX; d++) ar[d] = ai[d] = 0.0;
-    for (long long row = (long long)blockIdx.x * LR_ROWBLK + threadIdx.x; row < rows;
-         row += (long long)gridDim.x * LR_ROWBLK) {
-        const int i = (int)(row / g.ny), j = (int)(row % g.ny);
-        const double x = g.xmin + (i + 0.5) * g.dx - xc;
+    if (j < g.ny) {
+        const long long row = (long long)i * g.ny + j;
+        const double x = g.xmin + (i + g.ioff + 0.5) * g.dx - xc;
         const double y = g.ymin + (j + 0.5) * g.dy - yc;
         const double rho2 = x * x + y * y;
         double smr = 1.0, smi = 0.0;      // Q_m^m
@@ -302,18 +305,18 @@ __global__ void __launch_bounds__(LR_ROWBLK) lmax_rows(GravArgs a, const double 
             double s = 0.0;
             for (int w = 0; w < NW; w++) s += red[w][q];
             const double f = c_norm[l * (LM_MAX + 1) + m] * (g.dx * g.dy * g.dz);
-            a.scratch[(long long)blockIdx.x * LM_NC + l * l + l + ((q & 1) ? -m : m)] = f * s;
+            parts[(long long)blockIdx.x * LM_NC + l * l + l + ((q & 1) ? -m : m)] = f * s;
         }
     }
 }
 
 // one warp per coefficient: the blocks' partials, lane-strided, then a fixed
 // butterfly (deterministic)
-__global__ void __launch_bounds__(32) lmax_final(GravArgs a, int nparts)
+__global__ void __launch_bounds__(32) lmax_final(GravArgs a, const double *parts, int nparts)
 {
     const int t = blockIdx.x, lane = threadIdx.x;
     double s = 0.0;
-    for (int b = lane; b < nparts; b += 32) s += a.scratch[(long long)b * LM_NC + t];
+    for (int b = lane; b < nparts; b += 32) s += parts[(long long)b * LM_NC + t];
     s = warp_sum(s);
     if (lane == 0) a.mom[4 + t] = s;
     if (t == 0 && lane < 4) a.mom[lane] = a.sc->moments[lane];
@@ -350,10 +353,11 @@ __global__ void boundary_lmax_kernel(GravArgs a)
     if (t >= nb) return;
     int i, j, k;
     boundary_cell(t, g.nx, g.ny, g.nz, zb, i, j, k);
-    double x = g.xmin + (i + 0.5) * g.dx, y = g.ymin + (j + 0.5) * g.dy, z = g.zmin + (k + 0.5) * g.dz;
+    if (i < g.olo || i >= g.ohi) return;   // a ghost plane: the neighbour's cells
+    double x = g.xmin + (i + g.ioff + 0.5) * g.dx, y = g.ymin + (j + 0.5) * g.dy, z = g.zmin + (k + 0.5) * g.dz;
     if (zb && (k == 0 || k == g.nz - 1)) z = (k == g.nz - 1) ? g.zmax - 0.5 * g.dz : g.zmin + 0.5 * g.dz;
     else if (j == 0 || j == g.ny - 1) y = (j == g.ny - 1) ? g.ymax - 0.5 * g.dy : g.ymin + 0.5 * g.dy;
-    else x = (i == g.nx - 1) ? g.xmax - 0.5 * g.dx : g.xmin + 0.5 * g.dx;
+    else x = (i + g.ioff == g.gnx - 1) ? g.xmax - 0.5 * g.dx : g.xmin + 0.5 * g.dx;
     a.phi[((long long)i * g.ny + j) * g.nz + k] = eval_lmax(x, y, z, a.lmax, a.mom, a.G);
 }
 
@@ -383,45 +387,79 @@ cudaError_t ensure_norm()
 
 }  // namespace
 
-// centre of mass, the rows' z-power sums about it, then the solid-harmonic
-// moments row by row.  Scratch: partial sums at [0, LM_SCRATCH0), the z-power
-// sums (lmax + 1 per row) after it.
-cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
+// Row blocks per plane of lmax_rows.
+static int rows_per_plane_blocks(const Geom &g) { return (g.ny + LR_ROWBLK - 1) / LR_ROWBLK; }
+
+// Partial sums of the moment passes, per plane: 9 doubles (tree order of
+// the quadrupole moments) or rows_per_plane_blocks x LM_NC (lmax rows).
+static long long part_cap(const Geom &g)
+{
+    return std::max<long long>(64 * 1024, (long long)g.nx * rows_per_plane_blocks(g) * LM_NC);
+}
+
+long long grav_scratch_len(const Geom &g) { return part_cap(g) + (long long)g.nx * g.ny * (LM_MAX + 1); }
+
+int lmax_slab_width(const Geom &g) { return rows_per_plane_blocks(g) * LM_NC; }
+
+// Pass 0: the centre-of-mass partials of the own planes; pass 1: the rows'
+// z-power sums about the centre of mass (in the scratch after the partials),
+// then the harmonic partials of the own planes' row blocks.
+cudaError_t grav_moments_lmax_parts(const GravArgs &a, int pass, double *parts, cudaStream_t s)
 {
     if (a.lmax < 1 || a.lmax > LM_MAX) return cudaErrorInvalidValue;
-    const long long rows = (long long)a.g.nx * a.g.ny;
-    if (a.scratch_len < LM_SCRATCH0 + rows * (LM_MAX + 1)) return cudaErrorInvalidValue;
+    const int np = a.g.ohi - a.g.olo;
+    if (np <= 0 || a.scratch_len < grav_scratch_len(a.g)) return cudaErrorInvalidValue;
     cudaError_t e = ensure_norm();
     if (e != cudaSuccess) return e;
-    constexpr int NCOM = 592;   // 4 CTAs of 8 warps per SM
-    lmax_com_partial<<<NCOM, LR_NT, 0, s>>>(a);
-    lmax_com_final<<<1, 128, 0, s>>>(a, NCOM);
+    if (pass == 0) {
+        lmax_com_partial<<<np, LR_NT, 0, s>>>(a, parts);
+        return cudaGetLastError();
+    }
     const double *com = a.sc->moments + 1;
-    double *zs = a.scratch + LM_SCRATCH0;
+    double *zs = a.scratch + part_cap(a.g);
+    const long long rows = (long long)np * a.g.ny;
     const int nzb = (int)std::min<long long>((rows + LR_NT / 32 - 1) / (LR_NT / 32), 148LL * 8);
-    const int nb = (int)std::min<long long>((rows + LR_ROWBLK - 1) / LR_ROWBLK, LM_SCRATCH0 / LM_NC);
+    const int nb = np * rows_per_plane_blocks(a.g);
     auto launch = [&](auto zk, auto rk) -> cudaError_t {
         zk<<<nzb, LR_NT, 0, s>>>(a, com, zs);
-        rk<<<dim3(nb, a.lmax + 1), LR_ROWBLK, 0, s>>>(a, com, zs);
+        rk<<<dim3(nb, a.lmax + 1), LR_ROWBLK, 0, s>>>(a, com, zs, parts);
         return cudaGetLastError();
     };
     switch (a.lmax) {
-    case 1: e = launch(lmax_zsums<1>, lmax_rows<1>); break;
-    case 2: e = launch(lmax_zsums<2>, lmax_rows<2>); break;
-    case 3: e = launch(lmax_zsums<3>, lmax_rows<3>); break;
-    case 4: e = launch(lmax_zsums<4>, lmax_rows<4>); break;
-    case 5: e = launch(lmax_zsums<5>, lmax_rows<5>); break;
-    case 6: e = launch(lmax_zsums<6>, lmax_rows<6>); break;
-    case 7: e = launch(lmax_zsums<7>, lmax_rows<7>); break;
-    case 8: e = launch(lmax_zsums<8>, lmax_rows<8>); break;
-    case 9: e = launch(lmax_zsums<9>, lmax_rows<9>); break;
-    case 10: e = launch(lmax_zsums<10>, lmax_rows<10>); break;
-    case 11: e = launch(lmax_zsums<11>, lmax_rows<11>); break;
-    default: e = launch(lmax_zsums<12>, lmax_rows<12>); break;
+    case 1: return launch(lmax_zsums<1>, lmax_rows<1>);
+    case 2: return launch(lmax_zsums<2>, lmax_rows<2>);
+    case 3: return launch(lmax_zsums<3>, lmax_rows<3>);
+    case 4: return launch(lmax_zsums<4>, lmax_rows<4>);
+    case 5: return launch(lmax_zsums<5>, lmax_rows<5>);
+    case 6: return launch(lmax_zsums<6>, lmax_rows<6>);
+    case 7: return launch(lmax_zsums<7>, lmax_rows<7>);
+    case 8: return launch(lmax_zsums<8>, lmax_rows<8>);
+    case 9: return launch(lmax_zsums<9>, lmax_rows<9>);
+    case 10: return launch(lmax_zsums<10>, lmax_rows<10>);
+    case 11: return launch(lmax_zsums<11>, lmax_rows<11>);
+    default: return launch(lmax_zsums<12>, lmax_rows<12>);
     }
-    if (e != cudaSuccess) return e;
-    lmax_final<<<(a.lmax + 1) * (a.lmax + 1), 32, 0, s>>>(a, nb);
+}
+
+// parts: the partials of nplanes planes of the whole grid, in plane order.
+cudaError_t grav_moments_lmax_set(const GravArgs &a, int pass, const double *parts, int nplanes, cudaStream_t s)
+{
+    if (pass == 0) lmax_com_final<<<1, 128, 0, s>>>(a, parts, nplanes);
+    else lmax_final<<<(a.lmax + 1) * (a.lmax + 1), 32, 0, s>>>(a, parts, nplanes * rows_per_plane_blocks(a.g));
     return cudaGetLastError();
+}
+
+// The centre of mass, the rows' z-power sums about it, then the
+// solid-harmonic moments row by row, each from per-plane partials added in
+// plane order.
+cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s)
+{
+    const int np = a.g.ohi - a.g.olo;
+    cudaError_t e = grav_moments_lmax_parts(a, 0, a.scratch, s);
+    if (e == cudaSuccess) e = grav_moments_lmax_set(a, 0, a.scratch, np, s);
+    if (e == cudaSuccess) e = grav_moments_lmax_parts(a, 1, a.scratch, s);
+    if (e == cudaSuccess) e = grav_moments_lmax_set(a, 1, a.scratch, np, s);
+    return e;
 }
 
 cudaError_t grav_boundary_lmax(const GravArgs &a, cudaStream_t s)

@@ -36,6 +36,11 @@ struct Geom {
     long long n;               // nx*ny*nz
     double xmin, xmax, ymin, ymax, zmin, zmax;
     double dx, dy, dz;         // (max-min)/n, hydro_solver_3d.c:55-57
+    // A slab of a grid split along x: the context holds global planes
+    // [ioff, ioff + nx) of gnx; its own planes are local [olo, ohi), the
+    // others ghost copies of a neighbour's.  xmin/xmax/dx are then the whole
+    // grid's, x = xmin + (i + ioff + 0.5) dx.  A whole grid: 0, nx, 0, nx.
+    int ioff, gnx, olo, ohi;
 };
 
 // Bitwise-ordered atomic max of a non-negative double (the bit pattern of a
@@ -180,6 +185,16 @@ struct GravArgs {
 // FP64 gravity (bit-exact) -- gravity_fp64.cu
 cudaError_t grav_moments_sequential(const GravArgs &a, cudaStream_t s);
 cudaError_t grav_moments_tree(const GravArgs &a, cudaStream_t s);
+// Moments of a slab (own planes [a.g.olo, a.g.ohi)).  Sequential order:
+// pass 0 / 1 continues the sums acc[0..4) / acc[0..9) (device memory) over
+// the own planes in cell order; grav_moments_seq_set stores the finished
+// sums (pass 0: M and the centre of mass; pass 1: Q).  Tree order: one
+// partial (9 doubles) per own plane into parts; grav_moments_tree_set adds
+// nparts partials of the whole grid in plane order.
+cudaError_t grav_moments_seq_slab(const GravArgs &a, int pass, double *acc, cudaStream_t s);
+cudaError_t grav_moments_seq_set(const GravArgs &a, int pass, const double *acc, cudaStream_t s);
+cudaError_t grav_moments_tree_parts(const GravArgs &a, int pass, double *parts, cudaStream_t s);
+cudaError_t grav_moments_tree_set(const GravArgs &a, int pass, const double *parts, int nparts, cudaStream_t s);
 cudaError_t grav_boundary_ref(const GravArgs &a, cudaStream_t s);
 cudaError_t grav_boundary_periodic(const GravArgs &a, cudaStream_t s);
 cudaError_t grav_sor_color(const GravArgs &a, int color, int iter, cudaStream_t s);
@@ -193,6 +208,17 @@ cudaError_t grav_reset_slots(const GravArgs &a, int from, int count, cudaStream_
 cudaError_t grav_moments_lmax(const GravArgs &a, cudaStream_t s);
 cudaError_t grav_boundary_lmax(const GravArgs &a, cudaStream_t s);
 int lmax_ncoef(int lmax);
+// Moment scratch of a context (doubles): per-plane partials, then the rows'
+// z-power sums.
+long long grav_scratch_len(const Geom &g);
+// lmax moments of a slab: pass 0 writes one centre-of-mass partial (4
+// doubles) per own plane, pass 1 the rows' harmonic partials
+// (lmax_slab_width per own plane); grav_moments_lmax_set adds the partials
+// of nplanes planes of the whole grid in plane order (pass 0: M and the centre of
+// mass; pass 1: the coefficients).
+int lmax_slab_width(const Geom &g);
+cudaError_t grav_moments_lmax_parts(const GravArgs &a, int pass, double *parts, cudaStream_t s);
+cudaError_t grav_moments_lmax_set(const GravArgs &a, int pass, const double *parts, int nplanes, cudaStream_t s);
 
 }  // namespace hc
 

@@ -379,11 +379,53 @@ int hc_sor_solve_noalloc(double *phi, const double *rho, int nx, int ny, int nz,
  * replaces it (a value another slab of the same precision produced).
  * hc_copy_planes copies planes [i0, i0+count) of the 5 state fields to
  * (to_ctx = 0) or from (to_ctx = 1) a device buffer laid out field by field
- * (5 x count x ny x nz words of the context's precision).  Hydro only: with
- * self-gravity (G > 0) the Poisson solve is not decomposed. */
+ * (5 x count x ny x nz words of the context's precision).  With self-gravity
+ * (G > 0) each context is also declared a slab (hc_set_slab) and the
+ * Poisson solve runs across the slabs before each step, as below. */
 int hc_get_signal_speed(hc_ctx *ctx, double *s);
 int hc_set_signal_speed(hc_ctx *ctx, double s);
 int hc_copy_planes(hc_ctx *ctx, int i0, int count, void *dev_buf, int to_ctx);
+
+/* Self-gravity across slabs (FP64 contexts, isolated boundary, ny, nz >= 3;
+ * the whole grid's gravity_solve_potential, gravity_solver_3d.c:510-747).
+ * hc_set_slab declares that the context holds global planes
+ * [ioff, ioff + nx) of a grid of gnx planes: its config's xmin/xmax are the
+ * whole grid's (dx = (xmax - xmin) / gnx unless given), its own planes are
+ * all but the ghost planes (local 0 when ioff > 0, local nx-1 when
+ * ioff + nx < gnx), x faces exist only at global planes 0 and gnx-1, and
+ * hc_step no longer solves: its source term uses the potential of the last
+ * converged slab solve.  One solve, every step before hc_step, all slabs in
+ * lock step:
+ *   1. moments, pass 0 then pass 1.  hc_slab_moment_layout gives the form:
+ *      sequential (lmax 0 with HC_MOMENTS_SEQUENTIAL): hc_slab_moments
+ *      continues `width` sums in buf over the own planes (the first slab
+ *      starts from zeros, each next slab from the previous slab's result),
+ *      and every slab passes the last slab's sums to hc_slab_set_moments --
+ *      the reference's sums bit for bit; otherwise hc_slab_moments writes
+ *      `width` doubles per own plane and every slab passes all slabs'
+ *      partials, concatenated in plane order (gnx planes), to
+ *      hc_slab_set_moments -- the single context's tree order bit for bit;
+ *   2. hc_slab_sor_begin;
+ *   3. for iter = 0, 1, ... < max_iter: hc_slab_sor_sweep(iter, 0) and
+ *      (iter, 1) -- the whole grid's red and black colours -- each followed
+ *      by the ghost exchange of the potential (hc_slab_phi_planes: planes of
+ *      the colour-split potential, both colours, [2][count][ny (nz+1)/2]
+ *      doubles); after iteration 0 also hc_slab_sor_boundary and an
+ *      exchange; then the maximum over the slabs of hc_slab_sor_norm(iter)
+ *      -- stop with iter + 1 iterations when it is below tol;
+ *   4. hc_slab_sor_end(iterations, that maximum, converged).
+ * The result equals the single context's solve bit for bit (potential,
+ * iterations, residual). */
+int hc_set_slab(hc_ctx *ctx, int gnx, int ioff);
+int hc_slab_moment_layout(hc_ctx *ctx, int pass, int *sequential, int *width);
+int hc_slab_moments(hc_ctx *ctx, int pass, double *buf);
+int hc_slab_set_moments(hc_ctx *ctx, int pass, const double *all, int nplanes);
+int hc_slab_sor_begin(hc_ctx *ctx);
+int hc_slab_sor_sweep(hc_ctx *ctx, int iter, int colour);
+int hc_slab_sor_boundary(hc_ctx *ctx);
+int hc_slab_sor_norm(hc_ctx *ctx, int iter, double *norm);
+int hc_slab_sor_end(hc_ctx *ctx, int iterations, double residual, int converged);
+int hc_slab_phi_planes(hc_ctx *ctx, int i0, int count, void *buf, int to_ctx);
 
 /* Page-lock (pin) a host buffer for faster transfers, and release it. */
 int hc_host_register(void *ptr, size_t bytes);

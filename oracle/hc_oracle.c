@@ -149,53 +149,65 @@ double hco_cfl_dt(hco_grid *g)
 /* Gravity                                                                   */
 /* ------------------------------------------------------------------------ */
 
-/* gravity_solver_3d.c:164-262: sequential sums over cells with rho > 0. */
-void hco_moments_ref(const hco_grid *g, const double *rho, double *out)
+/* gravity_solver_3d.c:164-262: sequential sums over cells with rho > 0, in
+ * (i,j,k) order over the local planes [i0, i1), continuing the sums in acc.
+ * The grid holds global planes [ioff, ioff + nx); xmin and dx are the whole
+ * grid's, so x = xmin + (i + ioff + 0.5) dx is the whole grid's coordinate
+ * bit for bit.  pass 0: acc[0..3] = (M, sum dm x, sum dm y, sum dm z);
+ * pass 1: acc[0..8] = Q_ij about com[0..2]. */
+void hco_moments_acc(const hco_grid *g, const double *rho, int pass, int i0, int i1, int ioff,
+                     const double *com, double *acc)
 {
     const double dV = g->dx * g->dy * g->dz;
-    double M = 0.0, Mx = 0.0, My = 0.0, Mz = 0.0;
-    for (int i = 0; i < g->nx; i++)
+    for (int i = i0; i < i1; i++)
         for (int j = 0; j < g->ny; j++)
             for (int k = 0; k < g->nz; k++) {
                 double r = rho[at(g, i, j, k)];
-                if (r > 0.0) {
-                    double x = g->xmin + (i + 0.5) * g->dx;
+                if (!(r > 0.0)) continue;
+                double dm = r * dV;
+                if (pass == 0) {
+                    double x = g->xmin + (i + ioff + 0.5) * g->dx;
                     double y = g->ymin + (j + 0.5) * g->dy;
                     double z = g->zmin + (k + 0.5) * g->dz;
-                    double dm = r * dV;
-                    M += dm; Mx += dm * x; My += dm * y; Mz += dm * z;
-                }
-            }
-    double xc, yc, zc;
-    if (M > 0.0) { xc = Mx / M; yc = My / M; zc = Mz / M; }
-    else {
-        xc = 0.5 * (g->xmin + g->xmax);
-        yc = 0.5 * (g->ymin + g->ymax);
-        zc = 0.5 * (g->zmin + g->zmax);
-    }
-    double Q[9] = { 0 };
-    for (int i = 0; i < g->nx; i++)
-        for (int j = 0; j < g->ny; j++)
-            for (int k = 0; k < g->nz; k++) {
-                double r = rho[at(g, i, j, k)];
-                if (r > 0.0) {
-                    double x = g->xmin + (i + 0.5) * g->dx - xc;
-                    double y = g->ymin + (j + 0.5) * g->dy - yc;
-                    double z = g->zmin + (k + 0.5) * g->dz - zc;
-                    double dm = r * dV;
+                    acc[0] += dm; acc[1] += dm * x; acc[2] += dm * y; acc[3] += dm * z;
+                } else {
+                    double x = g->xmin + (i + ioff + 0.5) * g->dx - com[0];
+                    double y = g->ymin + (j + 0.5) * g->dy - com[1];
+                    double z = g->zmin + (k + 0.5) * g->dz - com[2];
                     double r2 = x * x + y * y + z * z;
-                    Q[0] += dm * (3.0 * x * x - r2);
-                    Q[1] += dm * (3.0 * x * y);
-                    Q[2] += dm * (3.0 * x * z);
-                    Q[3] += dm * (3.0 * y * x);
-                    Q[4] += dm * (3.0 * y * y - r2);
-                    Q[5] += dm * (3.0 * y * z);
-                    Q[6] += dm * (3.0 * z * x);
-                    Q[7] += dm * (3.0 * z * y);
-                    Q[8] += dm * (3.0 * z * z - r2);
+                    acc[0] += dm * (3.0 * x * x - r2);
+                    acc[1] += dm * (3.0 * x * y);
+                    acc[2] += dm * (3.0 * x * z);
+                    acc[3] += dm * (3.0 * y * x);
+                    acc[4] += dm * (3.0 * y * y - r2);
+                    acc[5] += dm * (3.0 * y * z);
+                    acc[6] += dm * (3.0 * z * x);
+                    acc[7] += dm * (3.0 * z * y);
+                    acc[8] += dm * (3.0 * z * z - r2);
                 }
             }
-    out[0] = M; out[1] = xc; out[2] = yc; out[3] = zc;
+}
+
+/* Centre of mass from the pass-0 sums (gravity_solver_3d.c:205-215): the
+ * box centre when there is no mass. */
+void hco_moments_com(const hco_grid *g, const double *acc, double *com)
+{
+    const double M = acc[0];
+    if (M > 0.0) { com[0] = acc[1] / M; com[1] = acc[2] / M; com[2] = acc[3] / M; }
+    else {
+        com[0] = 0.5 * (g->xmin + g->xmax);
+        com[1] = 0.5 * (g->ymin + g->ymax);
+        com[2] = 0.5 * (g->zmin + g->zmax);
+    }
+}
+
+void hco_moments_ref(const hco_grid *g, const double *rho, double *out)
+{
+    double acc[4] = { 0 }, com[3], Q[9] = { 0 };
+    hco_moments_acc(g, rho, 0, 0, g->nx, 0, NULL, acc);
+    hco_moments_com(g, acc, com);
+    hco_moments_acc(g, rho, 1, 0, g->nx, 0, com, Q);
+    out[0] = acc[0]; out[1] = com[0]; out[2] = com[1]; out[3] = com[2];
     memcpy(out + 4, Q, sizeof Q);
 }
 
@@ -246,23 +258,36 @@ void hco_boundary(hco_grid *g, const double *rho)
     }
     double mom[13];
     hco_moments_ref(g, rho, mom);
+    hco_boundary_mom(g, mom, 0, nx, 0, nx);
+}
+
+/* The monopole + quadrupole face loops of apply_boundary_conditions
+ * (gravity_solver_3d.c:302-498) over the local planes [i0, i1) of a grid
+ * that holds global planes [ioff, ioff + nx) of gnx: the x faces where the
+ * global planes 0 and gnx - 1 are held, then the y and z faces of those
+ * planes, in the reference's order (later faces overwrite shared edges). */
+void hco_boundary_mom(hco_grid *g, const double *mom, int ioff, int gnx, int i0, int i1)
+{
+    const int nx = g->nx, ny = g->ny, nz = g->nz;
+    double *phi = g->phi;
     const double G = g->G;
+    const int xlo = ioff == 0 && i0 == 0, xhi = ioff + nx == gnx && i1 == nx;
     for (int j = 0; j < ny; j++)
         for (int k = 0; k < nz; k++) {
             double y = g->ymin + (j + 0.5) * g->dy, z = g->zmin + (k + 0.5) * g->dz;
-            phi[at(g, 0, j, k)] = mono_quad(g->xmin + 0.5 * g->dx, y, z, mom, G);
-            phi[at(g, nx - 1, j, k)] = mono_quad(g->xmax - 0.5 * g->dx, y, z, mom, G);
+            if (xlo) phi[at(g, 0, j, k)] = mono_quad(g->xmin + 0.5 * g->dx, y, z, mom, G);
+            if (xhi) phi[at(g, nx - 1, j, k)] = mono_quad(g->xmax - 0.5 * g->dx, y, z, mom, G);
         }
-    for (int i = 0; i < nx; i++)
+    for (int i = i0; i < i1; i++)
         for (int k = 0; k < nz; k++) {
-            double x = g->xmin + (i + 0.5) * g->dx, z = g->zmin + (k + 0.5) * g->dz;
+            double x = g->xmin + (i + ioff + 0.5) * g->dx, z = g->zmin + (k + 0.5) * g->dz;
             phi[at(g, i, 0, k)] = mono_quad(x, g->ymin + 0.5 * g->dy, z, mom, G);
             phi[at(g, i, ny - 1, k)] = mono_quad(x, g->ymax - 0.5 * g->dy, z, mom, G);
         }
     if (nz > 1)
-        for (int i = 0; i < nx; i++)
+        for (int i = i0; i < i1; i++)
             for (int j = 0; j < ny; j++) {
-                double x = g->xmin + (i + 0.5) * g->dx, y = g->ymin + (j + 0.5) * g->dy;
+                double x = g->xmin + (i + ioff + 0.5) * g->dx, y = g->ymin + (j + 0.5) * g->dy;
                 phi[at(g, i, j, 0)] = mono_quad(x, y, g->zmin + 0.5 * g->dz, mom, G);
                 phi[at(g, i, j, nz - 1)] = mono_quad(x, y, g->zmax - 0.5 * g->dz, mom, G);
             }
@@ -439,6 +464,17 @@ static double sor_factor(const hco_grid *g, double *ix2, double *iy2, double *iz
     *iy2 = 1.0 / (g->dy * g->dy);
     *iz2 = 1.0 / (g->dz * g->dz);
     return g->nz == 1 ? 2.0 * (*ix2 + *iy2) : 2.0 * (*ix2 + *iy2 + *iz2);
+}
+
+/* One half sweep of local colour `colour` (cells with (i + j + k) % 2 ==
+ * colour in local indices) with the grid's coefficients; returns its update
+ * norm.  A slab whose first plane is global plane ioff sweeps the whole
+ * grid's colour c as local colour c ^ (ioff & 1). */
+double hco_sor_half(hco_grid *g, const double *rho, int colour)
+{
+    double ix2, iy2, iz2;
+    double fac = sor_factor(g, &ix2, &iy2, &iz2);
+    return sor_color(g, rho, colour, ix2, iy2, iz2, 4.0 * M_PI * g->G, fac);
 }
 
 /* gravity_solve_potential, gravity_solver_3d.c:510-747.  The boundary is
@@ -705,21 +741,24 @@ static cons_t plm_flux(const hco_grid *g, const double *pl, size_t cl, size_t cr
     return hllc(cons_of_arr(L, g->gamma), cons_of_arr(R, g->gamma), a, g->gamma);
 }
 
-static int step_impl(hco_grid *g, double dt_given);
+static int step_impl(hco_grid *g, double dt_given, int solve);
 
-int hco_step(hco_grid *g) { return step_impl(g, 0.0); }
+int hco_step(hco_grid *g) { return step_impl(g, 0.0, 1); }
 
-int hco_step_dt(hco_grid *g, double dt) { return step_impl(g, dt); }
+int hco_step_dt(hco_grid *g, double dt) { return step_impl(g, dt, 1); }
 
-static int step_impl(hco_grid *g, double dt_given)
+int hco_step_ext(hco_grid *g, double dt) { return step_impl(g, dt, 0); }
+
+static int step_impl(hco_grid *g, double dt_given, int solve)
 {
     const int nx = g->nx, ny = g->ny, nz = g->nz;
     const size_t n = (size_t)nx * ny * nz;
     const double gam = g->gamma;
     int st = 1;
 
-    /* solve_gravity_field, hydro_solver_3d.c:558-591 */
-    if (g->gravity) {
+    /* solve_gravity_field, hydro_solver_3d.c:558-591 (solve == 0: the caller
+     * solved, and g->gx/gy/gz hold the acceleration the source uses) */
+    if (g->gravity && solve) {
         double *rho = (double *)malloc(n * sizeof(double));
         memcpy(rho, g->q[0], n * sizeof(double));
         st = hco_gravity_solve(g, rho);

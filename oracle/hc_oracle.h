@@ -52,6 +52,9 @@ double hco_signal_max(const hco_grid *g);
 /* One step with a given dt instead of the grid's own CFL dt: a slab of a
  * larger grid steps with the whole grid's dt. */
 int hco_step_dt(hco_grid *g, double dt);
+/* The same without the gravity solve: the source term uses g->gx/gy/gz as
+ * they are (a slab whose potential was solved across all slabs). */
+int hco_step_ext(hco_grid *g, double dt);
 
 /* gravity_solve / gravity_solve_potential / gravity_compute_acceleration
  * (gravity_solver_3d.c:905, :510, :753). */
@@ -65,6 +68,23 @@ void hco_moments_ref(const hco_grid *g, const double *rho, double *out);
 
 /* apply_boundary_conditions (gravity_solver_3d.c:268-504) on g->phi. */
 void hco_boundary(hco_grid *g, const double *rho);
+
+/* Slabs (no reference counterpart; the reference steps one grid): a grid
+ * that holds global planes [ioff, ioff + nx) of a grid of gnx planes along
+ * x, with the whole grid's xmin, xmax and dx.
+ *   hco_moments_acc   the moment sums of compute_mass_moments (pass 0) or
+ *                     compute_quadrupole_moment (pass 1, about com) over the
+ *                     local planes [i0, i1), continuing acc -- slabs chained
+ *                     in plane order give the single grid's sums bit for bit;
+ *   hco_moments_com   the centre of mass from the pass-0 sums;
+ *   hco_boundary_mom  the monopole + quadrupole face values (mom as
+ *                     hco_moments_ref's out) on the local planes [i0, i1);
+ *   hco_sor_half      one half sweep of a local colour; its update norm. */
+void hco_moments_acc(const hco_grid *g, const double *rho, int pass, int i0, int i1, int ioff,
+                     const double *com, double *acc);
+void hco_moments_com(const hco_grid *g, const double *acc, double *com);
+void hco_boundary_mom(hco_grid *g, const double *mom, int ioff, int gnx, int i0, int i1);
+double hco_sor_half(hco_grid *g, const double *rho, int colour);
 
 /* Extension (no reference counterpart): multipole to degree lmax about the
  * centre of mass with real solid harmonics.  com[3]; cs[(lmax+1)^2] holds

@@ -76,6 +76,13 @@ def oracle_lib():
         lib.hco_residual_norm.restype = C.c_double
         lib.hco_sweep_norm.argtypes = [gp, _dp, _dp]
         lib.hco_sweep_norm.restype = C.c_double
+        lib.hco_step_ext.argtypes = [gp, C.c_double]
+        lib.hco_step_ext.restype = C.c_int
+        lib.hco_moments_acc.argtypes = [gp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]
+        lib.hco_moments_com.argtypes = [gp, _dp, _dp]
+        lib.hco_boundary_mom.argtypes = [gp, _dp, C.c_int, C.c_int, C.c_int, C.c_int]
+        lib.hco_sor_half.argtypes = [gp, _dp, C.c_int]
+        lib.hco_sor_half.restype = C.c_double
         _olib = lib
     return _olib
 

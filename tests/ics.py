@@ -63,3 +63,16 @@ def polytrope_n1(shape, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), M=1.0, R=0.35, G
     p = K * rho * rho
     z = np.zeros(shape)
     return prim_to_cons(rho, z, z, z, p, gamma), gamma
+
+
+def gravity_blob(shape, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """An off-centre n=1 polytrope (gamma = 2, G = 1) given a smooth shearing
+    velocity, so that the density and the potential change every step."""
+    q, gamma = polytrope_n1(shape, lo, hi, R=0.3, centre=(0.46, 0.53, 0.49))
+    X, Y, Z = centres(shape, lo, hi)
+    rho = q[0]
+    p = (gamma - 1.0) * q[4]
+    u = 0.2 * np.sin(2 * np.pi * Y)
+    v = 0.15 * np.cos(2 * np.pi * Z)
+    w = 0.1 * np.sin(2 * np.pi * X)
+    return prim_to_cons(rho, u, v, w, p, gamma)

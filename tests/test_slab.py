@@ -1,8 +1,11 @@
-"""The slab decomposition of the hydro step (hydrocode_astro1_b200/slab.py)
-on the CPU: slabs backed by the oracle, in one process and as gloo ranks of a
+"""The slab decomposition of the step (hydrocode_astro1_b200/slab.py) on the
+CPU: slabs backed by the oracle, in one process and as gloo ranks of a
 process group, step bit for bit as the oracle's single grid (state and every
-dt) -- the decomposition reproduces the reference's step exactly, since each
-slab's planes see the same neighbours and the same dt."""
+dt; with self-gravity also the potential, the SOR iteration count and the
+final update norm) -- the decomposition reproduces the reference's step
+exactly, since each slab's planes see the same neighbours and the same dt,
+the moment sums run in the reference's cell order across the slabs, and the
+red-black half sweeps see the same neighbour values."""
 import os
 import socket
 
@@ -17,6 +20,8 @@ from hydrocode_astro1_b200 import slab  # noqa: E402
 from slab_oracle import OracleSlab, gloo_worker  # noqa: E402
 
 BC = (1, 2, 2, 1, 1, 2)   # reflective and outflow faces, no periodic x
+GRAV = dict(G=1.0, gamma=2.0, cfl=0.3, omega=1.7, tol=1e-7, max_iter=3000)
+GBC = (2, 2, 2, 2, 2, 2)
 
 
 def single(shape, steps):
@@ -70,3 +75,68 @@ def test_gloo_ranks_match_single_grid(world, tmp_path):
     for r in range(world):
         assert np.array_equal(np.load(tmp_path / f"dt{r}.npy"), dts)
     assert np.array_equal(got, ref)
+
+
+def single_gravity(shape, steps):
+    q0 = ics.gravity_blob(shape)
+    o = OracleSim(*shape, bc=GBC, **GRAV)
+    o.set_state(q0)
+    d, its, res = o.step(steps)
+    return o.state(), o.phi.copy(), d, its, res
+
+
+@pytest.mark.parametrize("parts", [2, 3])
+def test_local_slabs_with_gravity_match_single_grid(parts):
+    """Three self-gravitating steps (the first solve from a zero potential,
+    the later ones warm-started); 17 planes in 3 slabs puts odd global
+    offsets on two of them."""
+    shape, steps = (17, 12, 14), 3
+    ref, phi, dts, its, res = single_gravity(shape, steps)
+    assert its.min() > 10   # every solve iterates
+    q0 = ics.gravity_blob(shape)
+    slabs = [OracleSlab(shape, e, bc=GBC, **GRAV) for e in slab.plan(shape[0], parts)]
+    for s in slabs:
+        s.set_state(q0)
+    comm = slab.LocalComm(slabs)
+    got_dt = [comm.step() for _ in range(steps)]
+    assert np.array_equal(np.array(got_dt), dts)
+    assert np.array_equal(np.concatenate([s.own_state() for s in slabs], axis=1), ref)
+    assert np.array_equal(np.concatenate([s.own_phi() for s in slabs], axis=0), phi)
+    for s in slabs:
+        assert s.o.g.last_iter == its[-1] and s.o.g.last_res == res[-1]
+
+
+def test_gravity_solve_stops_at_max_iter_like_single_grid():
+    """A solve capped below convergence: every slab reports the cap and the
+    last iteration's norm, and the step keeps the previous acceleration."""
+    shape, steps = (15, 11, 12), 2
+    kw = dict(GRAV, max_iter=6)
+    q0 = ics.gravity_blob(shape)
+    o = OracleSim(*shape, bc=GBC, **kw)
+    o.set_state(q0)
+    d, its, res = o.step(steps)
+    slabs = [OracleSlab(shape, e, bc=GBC, **kw) for e in slab.plan(shape[0], 2)]
+    for s in slabs:
+        s.set_state(q0)
+    comm = slab.LocalComm(slabs)
+    got_dt = [comm.step() for _ in range(steps)]
+    assert np.array_equal(np.array(got_dt), d)
+    assert np.array_equal(np.concatenate([s.own_state() for s in slabs], axis=1), o.state())
+    assert all(s.o.g.last_iter == 6 == its[-1] and s.o.g.last_res == res[-1] for s in slabs)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_with_gravity_match_single_grid(world, tmp_path):
+    shape, steps = (16, 10, 12), 2
+    ref, phi, dts, its, res = single_gravity(shape, steps)
+    torch.multiprocessing.spawn(gloo_worker,
+                                args=(world, free_port(), shape, steps, GBC, str(tmp_path), GRAV),
+                                nprocs=world, join=True)
+    got = np.concatenate([np.load(tmp_path / f"rank{r}.npy") for r in range(world)], axis=1)
+    got_phi = np.concatenate([np.load(tmp_path / f"phi{r}.npy") for r in range(world)], axis=0)
+    for r in range(world):
+        assert np.array_equal(np.load(tmp_path / f"dt{r}.npy"), dts)
+        it, rr = np.load(tmp_path / f"it{r}.npy")
+        assert it == its[-1] and rr == res[-1]
+    assert np.array_equal(got, ref)
+    assert np.array_equal(got_phi, phi)
