@@ -1659,7 +1659,11 @@ extern "C" int hc_slab_sor_end(hc_ctx *c, int iterations, double residual, int c
 }
 
 // Planes [i0, i0 + count) of the colour-split potential, both colours:
-// buf holds [2][count][ny * ((nz + 1) / 2)] doubles.
+// buf holds [2][count][ny * ((nz + 1) / 2)] doubles indexed by the whole
+// grid's colour.  The context's colour arrays are split by the local parity
+// (i + j + k) & 1, which is the global colour xor (ioff & 1); a row keeps the
+// same position k >> 1 in either, so slabs of either offset parity exchange
+// through the same buffer.
 extern "C" int hc_slab_phi_planes(hc_ctx *c, int i0, int count, void *buf, int to_ctx)
 {
     int rc = slab_ready(c);
@@ -1669,7 +1673,7 @@ extern "C" int hc_slab_phi_planes(hc_ctx *c, int i0, int count, void *buf, int t
     const size_t plane = (size_t)c->g.ny * ((c->g.nz + 1) / 2);
     const size_t cs = (size_t)c->g.nx * plane, bytes = (size_t)count * plane * sizeof(double);
     for (int q = 0; q < 2; q++) {
-        double *f = c->phs + q * cs + (size_t)i0 * plane;
+        double *f = c->phs + (q ^ (c->g.ioff & 1)) * cs + (size_t)i0 * plane;
         char *b = static_cast<char *>(buf) + q * bytes;
         CK(cudaMemcpyAsync(to_ctx ? (void *)f : (void *)b, to_ctx ? (const void *)b : (const void *)f, bytes,
                            cudaMemcpyDefault, c->s));

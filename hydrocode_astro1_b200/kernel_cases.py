@@ -2,6 +2,7 @@
 
     python -m hydrocode_astro1_b200.kernel_cases hydro N STEPS
     python -m hydrocode_astro1_b200.kernel_cases sor N ITERATIONS [SOR_DEPTH]
+    python -m hydrocode_astro1_b200.kernel_cases stream N
 
 `hydro`: the N^3 stellar explosion in FP32 with self-gravity, its Poisson
 solve capped at 2 iterations (it does not converge, so g stays the last
@@ -14,6 +15,11 @@ kernels, so an ncu capture of one of them starts at once.
 a cold start, each capped at ITERATIONS correction iterations; prints the
 second solve's colour sweeps' time per iteration and algorithmic bandwidth
 (6 bytes per interior cell and sweep).
+
+`stream`: the bandwidth a plain streaming kernel reaches for one colour
+sweep's transfer at N^3 -- three FP32 arrays of N^3/2 read, one written
+(torch.addcmul, a library kernel timed here only as a reference point for
+the sweep) -- 50 launches back to back, CUDA events around them.
 """
 from __future__ import annotations
 
@@ -61,11 +67,32 @@ def sor(n, iters, depth=0):
     s.close()
 
 
+def stream(n):
+    import torch
+    m = n * n * n // 2
+    x, y, z = (torch.rand(m, device="cuda") for _ in range(3))
+    out = torch.empty_like(x)
+    for _ in range(5):
+        torch.addcmul(x, y, z, out=out)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(50):
+        torch.addcmul(x, y, z, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    per = e0.elapsed_time(e1) / 50
+    print(f"stream n={n}: {per * 1e3:.1f} us per launch, {16 * m / (per * 1e-3) / 1e9:.0f} GB/s "
+          f"({16 * m / 1e6:.0f} MB per launch)", flush=True)
+
+
 if __name__ == "__main__":
     what = sys.argv[1]
     if what == "hydro":
         hydro(int(sys.argv[2]), int(sys.argv[3]))
     elif what == "sor":
         sor(int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4]) if len(sys.argv) > 4 else 0)
+    elif what == "stream":
+        stream(int(sys.argv[2]))
     else:
-        raise SystemExit("usage: kernel_cases hydro N STEPS | sor N ITERATIONS [SOR_DEPTH]")
+        raise SystemExit("usage: kernel_cases hydro N STEPS | sor N ITERATIONS [SOR_DEPTH] | stream N")

@@ -171,6 +171,7 @@ class GpuSlab:
         self.s.slab_sor_end(used, res, conv)
 
     def get_phi_planes(self, i0, count):
+        # [2][count][ny (nz+1)/2], indexed by the whole grid's colour
         t = self.torch.empty((2, count, self.ny * ((self.nz + 1) // 2)), dtype=self.torch.float64, device=self.dev)
         self.s.slab_phi_planes(i0, count, t.data_ptr(), False)
         return t

@@ -410,7 +410,7 @@ int hc_copy_planes(hc_ctx *ctx, int i0, int count, void *dev_buf, int to_ctx);
  *      (iter, 1) -- the whole grid's red and black colours -- each followed
  *      by the ghost exchange of the potential (hc_slab_phi_planes: planes of
  *      the colour-split potential, both colours, [2][count][ny (nz+1)/2]
- *      doubles); after iteration 0 also hc_slab_sor_boundary and an
+ *      doubles indexed by the whole grid's colour); after iteration 0 also hc_slab_sor_boundary and an
  *      exchange; then the maximum over the slabs of hc_slab_sor_norm(iter)
  *      -- stop with iter + 1 iterations when it is below tol;
  *   4. hc_slab_sor_end(iterations, that maximum, converged).
