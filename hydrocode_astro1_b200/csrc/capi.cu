@@ -1496,8 +1496,9 @@ static bool slab_sequential(const hc_ctx *c)
 // Doubles per own plane of a pass's partials (or, sequential, the sums).
 static int slab_width(const hc_ctx *c, int pass)
 {
-    if (c->cfg.lmax == 0) return pass == 0 ? 4 : 9;
-    return pass == 0 ? 4 : lmax_slab_width(c->g);
+    if (slab_sequential(c)) return pass == 0 ? 4 : 9;
+    if (c->cfg.lmax == 0) return 9;   // tree partials: 9 slots per plane in both passes
+    return lmax_slab_width(c->g, pass);
 }
 
 static int slab_ready(hc_ctx *c)

@@ -96,16 +96,19 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-// Centre of mass, one partial per own plane (CTA): (S0, x S0, y S0, S1) over
-// its rows, S0 = sum_k rho, S1 = sum_k rho z (cells with rho > 0, as in
-// every moment); warp w takes rows w, w + 8, ...
+// Centre of mass, COM_PP partials per own plane (one CTA each): (S0, x S0,
+// y S0, S1) over its rows, S0 = sum_k rho, S1 = sum_k rho z (cells with
+// rho > 0, as in every moment); warp w of part p takes rows
+// p * 8 + w, + 8 COM_PP, ...
+constexpr int COM_PP = 4;
+
 __global__ void __launch_bounds__(LR_NT) lmax_com_partial(GravArgs a, double *parts)
 {
     const Geom g = a.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = g.olo + blockIdx.x;
+    const int i = g.olo + (int)blockIdx.x / COM_PP, part = (int)blockIdx.x % COM_PP;
     double v0 = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
-    for (int j = warp; j < g.ny; j += LR_NT / 32) {
+    for (int j = part * (LR_NT / 32) + warp; j < g.ny; j += COM_PP * (LR_NT / 32)) {
         const long long base = ((long long)i * g.ny + j) * g.nz;
         double s0 = 0.0, s1 = 0.0;
         for (int k0 = 0; k0 < g.nz; k0 += 32 * LR_UNROLL) {
@@ -399,7 +402,7 @@ static long long part_cap(const Geom &g)
 
 long long grav_scratch_len(const Geom &g) { return part_cap(g) + (long long)g.nx * g.ny * (LM_MAX + 1); }
 
-int lmax_slab_width(const Geom &g) { return rows_per_plane_blocks(g) * LM_NC; }
+int lmax_slab_width(const Geom &g, int pass) { return pass == 0 ? 4 * COM_PP : rows_per_plane_blocks(g) * LM_NC; }
 
 // Pass 0: the centre-of-mass partials of the own planes; pass 1: the rows'
 // z-power sums about the centre of mass (in the scratch after the partials),
@@ -412,7 +415,7 @@ cudaError_t grav_moments_lmax_parts(const GravArgs &a, int pass, double *parts, 
     cudaError_t e = ensure_norm();
     if (e != cudaSuccess) return e;
     if (pass == 0) {
-        lmax_com_partial<<<np, LR_NT, 0, s>>>(a, parts);
+        lmax_com_partial<<<np * COM_PP, LR_NT, 0, s>>>(a, parts);
         return cudaGetLastError();
     }
     const double *com = a.sc->moments + 1;
@@ -444,7 +447,7 @@ cudaError_t grav_moments_lmax_parts(const GravArgs &a, int pass, double *parts, 
 // parts: the partials of nplanes planes of the whole grid, in plane order.
 cudaError_t grav_moments_lmax_set(const GravArgs &a, int pass, const double *parts, int nplanes, cudaStream_t s)
 {
-    if (pass == 0) lmax_com_final<<<1, 128, 0, s>>>(a, parts, nplanes);
+    if (pass == 0) lmax_com_final<<<1, 128, 0, s>>>(a, parts, nplanes * COM_PP);
     else lmax_final<<<(a.lmax + 1) * (a.lmax + 1), 32, 0, s>>>(a, parts, nplanes * rows_per_plane_blocks(a.g));
     return cudaGetLastError();
 }

@@ -211,12 +211,12 @@ int lmax_ncoef(int lmax);
 // Moment scratch of a context (doubles): per-plane partials, then the rows'
 // z-power sums.
 long long grav_scratch_len(const Geom &g);
-// lmax moments of a slab: pass 0 writes one centre-of-mass partial (4
-// doubles) per own plane, pass 1 the rows' harmonic partials
-// (lmax_slab_width per own plane); grav_moments_lmax_set adds the partials
-// of nplanes planes of the whole grid in plane order (pass 0: M and the centre of
-// mass; pass 1: the coefficients).
-int lmax_slab_width(const Geom &g);
+// lmax moments of a slab: pass 0 writes the centre-of-mass partials, pass 1
+// the rows' harmonic partials, lmax_slab_width(g, pass) doubles per own
+// plane; grav_moments_lmax_set adds the partials of nplanes planes of the
+// whole grid in plane order (pass 0: M and the centre of mass; pass 1: the
+// coefficients).
+int lmax_slab_width(const Geom &g, int pass);
 cudaError_t grav_moments_lmax_parts(const GravArgs &a, int pass, double *parts, cudaStream_t s);
 cudaError_t grav_moments_lmax_set(const GravArgs &a, int pass, const double *parts, int nplanes, cudaStream_t s);
 

@@ -333,10 +333,9 @@ cudaError_t forward(UNetState *u, const double *sumsq, cudaStream_t s)
 {
     const Dims *L = u->L;
     cudaError_t e;
-    // one thread per DK voxels along k; 128-thread blocks for the first (136
-    // registers: 64 packed accumulators), 256 for the last
+    // one thread per DK voxels along k, 128-thread blocks (136 registers: 64
+    // packed accumulators)
     const unsigned nfirst = (unsigned)std::min<long long>((L[0].n / DK + 127) / 128, 148LL * 12);
-    const unsigned ncol = (unsigned)std::min<long long>((L[0].n / DK + 255) / 256, 148LL * 8);
     conv_first_kernel<<<nfirst, 128, 0, s>>>(u->pooled, sumsq, L[0], wf_of(u, 0), bias_of(u, 0), u->e[0]);
     for (int l = 1; l <= NLEV; l++) {
         pool2_kernel<<<nblk(L[l].n * 2), 256, 0, s>>>(u->e[l - 1], u->p[l], L[l]);
@@ -348,8 +347,10 @@ cudaError_t forward(UNetState *u, const double *sumsq, cudaStream_t s)
         if ((e = conv_fwd(u, 2 * NLEV - l, u->sm[l], u->d[l], l, 0, s))) return e;
         h = u->d[l];
     }
-    conv_last_kernel<<<ncol, 256, 0, s>>>(u->d[0], L[0], wf_of(u, NCONV - 1), bias_of(u, NCONV - 1), u->out0);
-    return cudaGetLastError();
+    // the output convolution (16 -> 1 channel) on the tensor cores: the
+    // CUDA-core conv_last_kernel measured 283 us per 128^3 launch against
+    // ~80 us here
+    return conv_fwd(u, NCONV - 1, u->d[0], u->out0, 0, 2, s);
 }
 
 // gradients of the loss whose output gradient is in ga[0] (channel 0)

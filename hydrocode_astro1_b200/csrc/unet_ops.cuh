@@ -445,13 +445,13 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, 
 
 // master FP32 weights of one conv -> BF16 forward layout [co][tap][ci] and
 // input-gradient layout [ci][26-tap][co]
-// The network's first and last convolutions on the CUDA cores.  The first has
-// one input channel (the normalised pooled residual) and the last one output
-// channel: neither is a GEMM worth the tensor cores, whose kernel would pad
-// them to 16 channels.  A thread computes DK = 4 consecutive voxels along k of
-// one (i, j) row: for each of the 9 (di, dj) neighbour rows it reads the 6
-// voxels k0-1 .. k0+4 once and applies the 3 k taps to all 4 outputs.  The
-// weights of the tap in use sit in shared memory (read by broadcast); the
+// The network's first convolution on the CUDA cores.  It has one input
+// channel (the normalised pooled residual): not a GEMM worth the tensor
+// cores, whose kernel would pad it to 16 channels and read a padded input
+// volume.  A thread computes DK = 4 consecutive voxels along k of one (i, j)
+// row: for each of the 9 (di, dj) neighbour rows it reads the 6 voxels
+// k0-1 .. k0+4 once and applies the 3 k taps to all 4 outputs.  The weights
+// of the tap in use sit in shared memory (read by broadcast); the
 // multiply-adds are sm_100 packed FP32x2 operations.  The inputs are those of
 // the tensor-core path -- the same BF16 values -- and FP32 accumulation, in
 // another order, so outputs may differ from it in the last place.
@@ -527,56 +527,6 @@ __global__ void __launch_bounds__(128) conv_first_kernel(const float *__restrict
             st8(o, f0);
             st8(o + 8, f1);
         }
-    }
-}
-
-// out = conv(x) channel 0 + bias[0] (FP32, no activation): the network's
-// output from the 16 BF16 channels of x; zero padding.
-__global__ void __launch_bounds__(256) conv_last_kernel(const __nv_bfloat16 *__restrict__ x, Dims d,
-                                                        const __nv_bfloat16 *__restrict__ w,
-                                                        const float *__restrict__ bias, float *__restrict__ out)
-{
-    __shared__ float2 ws[NTAP][CH / 2];
-    for (int q = threadIdx.x; q < NTAP * CH; q += blockDim.x)
-        reinterpret_cast<float *>(&ws[q / CH][0])[q % CH] = __bfloat162float(w[q]);   // co = 0: w[tap][ci]
-    __syncthreads();
-    const float b0 = bias[0];
-    const int nkb = d.nz / DK;
-    const long long cols = (long long)nkb * d.ny * d.nx;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cols;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int kb = (int)(t % nkb);
-        const long long r = t / nkb;
-        const int j = (int)(r % d.ny), i = (int)(r / d.ny);
-        const int k0 = kb * DK;
-        float2 acc[DK];
-#pragma unroll
-        for (int kk = 0; kk < DK; kk++) acc[kk] = make_float2(0.f, 0.f);
-#pragma unroll 1
-        for (int dij = 0; dij < 9; dij++) {
-            const int a = i + dij / 3 - 1, b = j + dij % 3 - 1;
-            if (a < 0 || a >= d.nx || b < 0 || b >= d.ny) continue;
-            const __nv_bfloat16 *row = x + ((long long)a * d.ny + b) * d.nz * CH;
-#pragma unroll
-            for (int m = 0; m < DK + 2; m++) {
-                const int k = k0 - 1 + m;
-                if (k < 0 || k >= d.nz) continue;
-                float v[CH];
-                ld8(row + (long long)k * CH, *reinterpret_cast<float(*)[8]>(&v[0]));
-                ld8(row + (long long)k * CH + 8, *reinterpret_cast<float(*)[8]>(&v[8]));
-#pragma unroll
-                for (int dk = 0; dk < 3; dk++) {
-                    const int kk = m - dk;   // the output this neighbour feeds through tap dk
-                    if (kk < 0 || kk >= DK) continue;
-                    const float2 *wt = ws[dij * 3 + dk];
-#pragma unroll
-                    for (int c = 0; c < CH / 2; c++)
-                        acc[kk] = __ffma2_rn(make_float2(v[2 * c], v[2 * c + 1]), wt[c], acc[kk]);
-                }
-            }
-        }
-#pragma unroll
-        for (int kk = 0; kk < DK; kk++) out[vidx(d, i, j, k0 + kk)] = (acc[kk].x + acc[kk].y) + b0;
     }
 }
 
