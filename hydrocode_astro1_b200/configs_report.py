@@ -99,9 +99,15 @@ def blocks(values, size=BLOCK):
     return out
 
 
-def run(q0, p, precision, stop, warm=hc.HC_WARM_PREVIOUS, weights=None, max_steps=None, log=None, snap=None):
+PARTIAL_EVERY = 500
+
+
+def run(q0, p, precision, stop, warm=hc.HC_WARM_PREVIOUS, weights=None, max_steps=None, log=None, snap=None,
+        partial=None):
     """Steps until the stop rule holds; returns the final state and the
-    record (with snap = k, also the density at step k as rec["_snap"])."""
+    record (with snap = k, also the density at step k as rec["_snap"]).
+    partial(rec), when given, receives the record so far every
+    PARTIAL_EVERY steps (a run cut short keeps its blocks)."""
     kind, val = stop
     s = solver(p, precision, warm)
     if warm == hc.HC_WARM_UNET:
@@ -139,6 +145,9 @@ def run(q0, p, precision, stop, warm=hc.HC_WARM_PREVIOUS, weights=None, max_step
                 break
         if log and n % 100 == 0:
             log(f"  step {n}, t {t:.5f}, {time.time() - t0:.0f} s")
+        if partial and n % PARTIAL_EVERY == 0 and iters:
+            partial(dict(steps=n, t=t, wall_s=time.time() - t0, partial=True, sor_iterations_blocks=blocks(iters),
+                         sor_iterations_mean=float(np.mean(iters))))
     c1 = np.array(d_prev["cons"]) if n > 0 else c0
     q = s.state()
     d = s.diagnostics()
@@ -216,8 +225,12 @@ def main():
                 tag = arm if not unet or len(weights) == 1 else f"{arm}:{os.path.basename(wf)}"
                 log(f"[{name}] {tag}")
                 snap = rec["fp64"]["steps"] if (q64 is not None and capped) else None
+                def keep(part, tag=tag):
+                    rec[tag] = part
+                    save(out + [rec])
+
                 q32, r32 = run(q0, p, hc.FP32, fp32_stop, hc.HC_WARM_UNET if unet else hc.HC_WARM_PREVIOUS, wf,
-                               max_steps=a.max_steps, log=log, snap=snap)
+                               max_steps=a.max_steps, log=log, snap=snap, partial=keep)
                 rho_snap = r32.pop("_snap", None)
                 if q64 is not None and r32["steps"] == rec["fp64"]["steps"]:
                     r32["density_l1"] = float(np.abs(q32[0] - q64[0]).mean() / np.abs(q64[0]).mean())
