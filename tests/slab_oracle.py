@@ -117,7 +117,36 @@ class OracleSlab:
         return self.o.phi[self.olo:self.ohi].copy()
 
 
-def gloo_worker(rank, world, port, shape, steps, bc, out_dir, gravity=None):
+class TreeOracleSlab(OracleSlab):
+    """The oracle slab with the tree form of the moment protocol: one
+    partial per own plane (the reference's sums over that plane alone),
+    gathered from all slabs in plane order and added in plane order -- a
+    fixed order that any split of the planes reproduces."""
+
+    def moment_layout(self, p):
+        return False, (4 if p == 0 else 9)
+
+    def moments(self, p, buf):
+        w = 4 if p == 0 else 9
+        out = np.zeros((self.ohi - self.olo, w))
+        for i in range(self.olo, self.ohi):
+            acc = np.zeros(w)
+            self.o.lib.hco_moments_acc(C.byref(self.o.g), _ptr(self.o.q[0]), p, i, i + 1, self.ioff,
+                                       _ptr(self.com), _ptr(acc))
+            out[i - self.olo] = acc
+        return out.reshape(-1)
+
+    def set_moments(self, p, data, nplanes):
+        w = 4 if p == 0 else 9
+        parts = np.asarray(data, dtype=np.float64).reshape(nplanes, w)
+        acc = [0.0] * w
+        for row in parts:
+            for q in range(w):
+                acc[q] += float(row[q])
+        super().set_moments(p, np.array(acc), nplanes)
+
+
+def gloo_worker(rank, world, port, shape, steps, bc, out_dir, gravity=None, tree=False):
     """One rank of a gloo process group: its oracle slab of the smooth random
     flow (or, with gravity = dict of solver keywords, the polytrope-like
     self-gravitating blob) takes `steps` steps through ProcessGroupComm, then
@@ -140,7 +169,7 @@ def gloo_worker(rank, world, port, shape, steps, bc, out_dir, gravity=None):
         entry = slab.plan(shape[0], world)[rank]
         if gravity:
             q0 = ics.gravity_blob(shape)
-            sl = OracleSlab(shape, entry, bc=bc, **gravity)
+            sl = (TreeOracleSlab if tree else OracleSlab)(shape, entry, bc=bc, **gravity)
         else:
             q0 = ics.smooth_random(shape, seed=21)
             sl = OracleSlab(shape, entry, cfl=0.35, bc=bc)

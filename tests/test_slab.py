@@ -17,7 +17,7 @@ from oracle.oracle import OracleSim
 
 torch = pytest.importorskip("torch")
 from hydrocode_astro1_b200 import slab  # noqa: E402
-from slab_oracle import OracleSlab, gloo_worker  # noqa: E402
+from slab_oracle import OracleSlab, TreeOracleSlab, gloo_worker  # noqa: E402
 
 BC = (1, 2, 2, 1, 1, 2)   # reflective and outflow faces, no periodic x
 GRAV = dict(G=1.0, gamma=2.0, cfl=0.3, omega=1.7, tol=1e-7, max_iter=3000)
@@ -140,3 +140,29 @@ def test_gloo_ranks_with_gravity_match_single_grid(world, tmp_path):
         assert it == its[-1] and rr == res[-1]
     assert np.array_equal(got, ref)
     assert np.array_equal(got_phi, phi)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_tree_moments_match_one_slab(world, tmp_path):
+    """The tree form of the moment protocol (per-plane partials, gathered in
+    plane order with ProcessGroupComm.gather's padded all-gather, added in
+    plane order) as 2 and 3 gloo ranks against the same order on one slab
+    of the whole grid: state, potential, dt, iterations and final norm bit
+    for bit."""
+    shape, steps = (16, 10, 12), 2
+    q0 = ics.gravity_blob(shape)
+    one = TreeOracleSlab(shape, slab.plan(shape[0], 1)[0], bc=GBC, **GRAV)
+    one.set_state(q0)
+    comm = slab.LocalComm([one])
+    dts = [comm.step() for _ in range(steps)]
+    torch.multiprocessing.spawn(gloo_worker,
+                                args=(world, free_port(), shape, steps, GBC, str(tmp_path), GRAV, True),
+                                nprocs=world, join=True)
+    got = np.concatenate([np.load(tmp_path / f"rank{r}.npy") for r in range(world)], axis=1)
+    got_phi = np.concatenate([np.load(tmp_path / f"phi{r}.npy") for r in range(world)], axis=0)
+    for r in range(world):
+        assert np.array_equal(np.load(tmp_path / f"dt{r}.npy"), np.array(dts))
+        it, rr = np.load(tmp_path / f"it{r}.npy")
+        assert it == one.o.g.last_iter and rr == one.o.g.last_res
+    assert np.array_equal(got, one.own_state())
+    assert np.array_equal(got_phi, one.own_phi())
